@@ -1,0 +1,471 @@
+"""B200 LLG engine: the drop-in libgpukern C ABI, its fused extended ABI and
+the C++ restatement of the reference's Go driver, loaded through ctypes.
+
+Modules of this package:
+  * ``libgpukern.so``   -- CUDA kernels for sm_100a behind the reference's
+    libgpukern C ABI (include/gpukern.h) plus the fused ``mmx_*`` entry
+    points (include/mmx.h);
+  * ``libmmxdriver.so`` -- C++ host driver restating the Go driver over
+    any libgpukern implementation (include/mmx_driver.h).
+
+Nothing here falls back to a CPU path: if the CUDA library is missing the
+import fails with a message naming the build step.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "libgpukern.so")
+DRIVER_PATH = os.path.join(HERE, "libmmxdriver.so")
+
+SOLVERS = {"heun": 0, "rk12": 1, "rk23": 2, "rk4": 3, "rkck": 4, "rkdp": 5, "rk2": 6}
+ERRORS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "unsupported size", 4: "NaN", 5: "out of memory",
+          6: "bad state"}
+
+
+def build(jobs=8):
+    """Compile libgpukern.so and libmmxdriver.so in-tree for sm_100a."""
+    subprocess.check_call(["make", "-s", "-j%d" % jobs, "-f", os.path.join(HERE, "Makefile")], cwd=HERE)
+
+
+class MmxError(RuntimeError):
+    pass
+
+
+# --------------------------------------------------------------------------
+# ctypes prototypes
+# --------------------------------------------------------------------------
+c_float_p = ctypes.c_void_p
+c_int_p = ctypes.POINTER(ctypes.c_int)
+
+
+class MmxParams(ctypes.Structure):
+    _fields_ = [
+        ("size", ctypes.c_int * 3),
+        ("periodic", ctypes.c_int * 3),
+        ("cellsize", ctypes.c_float * 3),
+        ("alpha", ctypes.c_float),
+        ("hext", ctypes.c_float * 3),
+        ("anis_type", ctypes.c_int),
+        ("anis_k", ctypes.c_float),
+        ("anis_axis", ctypes.c_float * 3),
+        ("solver", ctypes.c_int),
+        ("dt", ctypes.c_float),
+        ("max_error", ctypes.c_float),
+        ("min_dm", ctypes.c_float),
+        ("max_dm", ctypes.c_float),
+        ("min_dt", ctypes.c_float),
+        ("max_dt", ctypes.c_float),
+        ("unit_time", ctypes.c_float),
+        ("exch_type", ctypes.c_int),
+        ("faithful", ctypes.c_int),
+        ("accuracy", ctypes.c_int),
+    ]
+
+
+class DriverConfig(ctypes.Structure):
+    _fields_ = [
+        ("grid", ctypes.c_int * 3),
+        ("cell", ctypes.c_double * 3),
+        ("periodic", ctypes.c_int * 3),
+        ("msat", ctypes.c_double),
+        ("aexch", ctypes.c_double),
+        ("alpha", ctypes.c_double),
+        ("bext", ctypes.c_double * 3),
+        ("anis_type", ctypes.c_int),
+        ("k1", ctypes.c_double),
+        ("anis_axis", ctypes.c_double * 3),
+        ("solver", ctypes.c_int),
+        ("dt", ctypes.c_double),
+        ("maxerror", ctypes.c_double),
+        ("mindm", ctypes.c_double),
+        ("maxdm", ctypes.c_double),
+        ("mindt", ctypes.c_double),
+        ("maxdt", ctypes.c_double),
+        ("faithful", ctypes.c_int),
+    ]
+
+
+# name -> (restype, argtypes); the libgpukern C ABI (include/gpukern.h)
+ABI = {
+    "gpu_init": (None, [ctypes.c_int, ctypes.c_int]),
+    "gpu_set_device": (None, [ctypes.c_int]),
+    "gpu_maxthreads": (ctypes.c_int, []),
+    "gpu_setmaxthreads": (None, [ctypes.c_int]),
+    "gpu_getproperties": (ctypes.c_void_p, []),
+    "gpu_print_properties_stdout": (None, []),
+    "gpu_getstream": (ctypes.c_void_p, []),
+    "gpu_init_stream": (None, []),
+    "new_gpu_array": (ctypes.c_void_p, [ctypes.c_int]),
+    "free_gpu_array": (None, [ctypes.c_void_p]),
+    "gpu_usedmem": (ctypes.c_ulonglong, []),
+    "gpu_stride_float": (ctypes.c_int, []),
+    "gpu_override_stride": (None, [ctypes.c_int]),
+    "memcpy_gpu_dir": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "memcpy_to_gpu": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "memcpy_from_gpu": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "memcpy_on_gpu": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "memcpy_on_gpu_async": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "gpu_array_get": (ctypes.c_float, [ctypes.c_void_p, ctypes.c_int]),
+    "gpu_array_set": (None, [ctypes.c_void_p, ctypes.c_int, ctypes.c_float]),
+    "gpu_zero": (None, [ctypes.c_void_p, ctypes.c_int]),
+    "gpu_zero_async": (None, [ctypes.c_void_p, ctypes.c_int]),
+    "assertHost": (None, [ctypes.c_void_p]),
+    "assertDevice": (None, [ctypes.c_void_p]),
+    "new_ram_array": (ctypes.c_void_p, [ctypes.c_int]),
+    "gpu_add": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "gpu_madd": (None, [ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_int]),
+    "gpu_madd2": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "gpu_add_constant": (None, [ctypes.c_void_p, ctypes.c_float, ctypes.c_int]),
+    "gpu_linear_combination": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_float,
+                                      ctypes.c_int]),
+    "gpu_linear_combination_many": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                           ctypes.c_int]),
+    "gpu_scale_dot_product": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float,
+                                     ctypes.c_int]),
+    "gpu_normalize_uniform": (None, [ctypes.c_void_p, ctypes.c_int]),
+    "gpu_normalize_map": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    "gpu_deltaM": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p, ctypes.c_float,
+                          ctypes.c_int]),
+    "gpu_add_local_fields": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
+    "gpu_add_local_fields_H_and_phi": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                              ctypes.c_void_p]),
+    "gpu_kernelmul6": (None, [ctypes.c_void_p] * 9 + [ctypes.c_int]),
+    "gpu_kernelmul4": (None, [ctypes.c_void_p] * 7 + [ctypes.c_int]),
+    "gpu_kernelmul3": (None, [ctypes.c_void_p] * 5 + [ctypes.c_int]),
+    "gpu_kernelmul_biot_savart3D": (None, [ctypes.c_void_p] * 6 + [ctypes.c_int]),
+    "gpu_kernelmul_biot_savart3DNx1": (None, [ctypes.c_void_p] * 5 + [ctypes.c_int]),
+    "gpu_kernelmul_biot_savart2D": (None, [ctypes.c_void_p] * 5 + [ctypes.c_int]),
+    "gpu_copy_pad": (None, [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 6),
+    "gpu_copy_unpad": (None, [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 6),
+    "gpu_copy_pad2D": (None, [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 4),
+    "gpu_copy_unpad2D": (None, [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 4),
+    "new_gpuFFT3dPlan_padded": (ctypes.c_void_p, [c_int_p, c_int_p]),
+    "new_gpuFFT3dPlan": (ctypes.c_void_p, [c_int_p]),
+    "delete_gpuFFT3dPlan": (None, [ctypes.c_void_p]),
+    "gpuFFT3dPlan_forward": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "gpuFFT3dPlan_inverse": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "gpuFFT3dPlan_normalization": (ctypes.c_int, [ctypes.c_void_p]),
+    "gpu_reduce": (ctypes.c_float, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_int]),
+    "gpu_partial_sums": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "gpu_partial_maxabs": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "gpu_add_exch": (None, [ctypes.c_void_p, ctypes.c_void_p, c_int_p, c_int_p, c_int_p, ctypes.c_void_p,
+                            ctypes.c_int]),
+    "gpu_add_lin_anisotropy": (None, [ctypes.c_void_p] * 12 + [ctypes.c_int]),
+    "gpu_anal_fw_step": (None, [ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_void_p]),
+    "gpu_spintorque_deltaM": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_float,
+                                     ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float,
+                                     ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "gpu_gaussian_noise": (None, [ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_int]),
+    "gpu_transpose_complex_YZ": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int]),
+    "gpu_transpose_complex_XZ": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int]),
+}
+
+MMX = {
+    "mmx_last_error": (ctypes.c_char_p, []),
+    "mmx_solver_create": (ctypes.c_int, [ctypes.POINTER(MmxParams), ctypes.POINTER(ctypes.c_void_p)]),
+    "mmx_solver_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "mmx_solver_set_m": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "mmx_solver_get_m": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "mmx_solver_normalize": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "mmx_solver_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "mmx_solver_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "mmx_solver_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                        ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_longlong)]),
+    "mmx_solver_set_hext": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "mmx_solver_m_device": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "mmx_solver_use_graph": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "mmx_solver_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "mmx_solver_pass_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                             ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
+                                             ctypes.POINTER(ctypes.c_int)]),
+    "mmx_face_kernel6": (ctypes.c_int, [c_int_p, c_int_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
+}
+
+DRIVER = {
+    "mmxd_last_error": (ctypes.c_char_p, []),
+    "mmxd_open": (ctypes.c_void_p, [ctypes.c_char_p]),
+    "mmxd_close": (None, [ctypes.c_void_p]),
+    "mmxd_new": (ctypes.c_void_p, [ctypes.c_void_p, ctypes.POINTER(DriverConfig), ctypes.c_void_p,
+                                   ctypes.c_void_p]),
+    "mmxd_free": (None, [ctypes.c_void_p]),
+    "mmxd_sizes": (None, [ctypes.c_void_p, c_int_p, c_int_p]),
+    "mmxd_internal": (None, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                             ctypes.c_void_p]),
+    "mmxd_steps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "mmxd_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "mmxd_get_m": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "mmxd_set_m": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "mmxd_heff": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "mmxd_avg_m": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "mmxd_time": (ctypes.c_double, [ctypes.c_void_p]),
+    "mmxd_dt": (ctypes.c_float, [ctypes.c_void_p]),
+    "mmxd_torque": (ctypes.c_float, [ctypes.c_void_p]),
+    "mmxd_step_count": (ctypes.c_longlong, [ctypes.c_void_p]),
+}
+
+_cache = {}
+
+
+def _load(path, table, tag):
+    if tag in _cache:
+        return _cache[tag]
+    if not os.path.exists(path):
+        raise ImportError("%s is not built: run __graft_entry__.build() (make -C 1_b200)" % path)
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in table.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _cache[tag] = lib
+    return lib
+
+
+def lib():
+    """The B200 libgpukern (ABI + mmx_*) with prototypes."""
+    t = dict(ABI)
+    t.update(MMX)
+    return _load(LIB_PATH, t, "gpukern")
+
+
+def driver():
+    return _load(DRIVER_PATH, DRIVER, "driver")
+
+
+def exported_symbols():
+    """Names the library must export (every declaration of include/*.h)."""
+    return sorted(list(ABI) + list(MMX))
+
+
+def _check(rc):
+    if rc != 0:
+        raise MmxError("%s: %s" % (ERRORS.get(rc, rc), lib().mmx_last_error().decode()))
+
+
+# --------------------------------------------------------------------------
+# Units and the user -> internal conversion (src/go/sim/material.go,
+# init.go, simgeom.go); float32 rounding at each step, as the Go code.
+# --------------------------------------------------------------------------
+def f32(x):
+    return np.float32(x)
+
+
+def units(msat, aexch):
+    mu0 = f32(4.0e-7 * np.pi)
+    gamma0 = f32(2.211e5)
+    ms, A = f32(msat), f32(aexch)
+    t = f32(f32(mu0 * ms) * ms)
+    L = f32(np.sqrt(2.0 * np.float64(f32(A / t))))
+    T = f32(f32(1.0) / f32(gamma0 * ms))
+    B = f32(mu0 * ms)
+    vol = f32(f32(L * L) * L)
+    E = f32(f32(A * L) / vol)
+    return dict(length=L, time=T, field=B, edens=E)
+
+
+def mmx_params(grid, cell, msat, aexch, alpha, bext=(0, 0, 0), solver="heun", dt=0.0, maxerror=0.0, anis=0,
+               k1=0.0, axis=(0, 0, 1), periodic=(0, 0, 0), faithful=1, exch_type=6):
+    """Builds mmx_params from the reference's user-level (SI, user x,y,z)
+    inputs with the same float32 conversions as the Go driver."""
+    u = units(msat, aexch)
+    p = MmxParams()
+    for d in range(3):
+        p.size[d] = grid[2 - d]
+        p.periodic[d] = periodic[2 - d]
+        p.cellsize[d] = f32(f32(cell[2 - d]) / u["length"])
+        p.hext[d] = f32(f32(bext[2 - d]) / u["field"])
+    p.alpha = f32(alpha)
+    p.anis_type = anis
+    if anis == 1:
+        p.anis_k = f32(f32(k1) / u["edens"])
+        ux, uy, uz = f32(axis[2]), f32(axis[1]), f32(axis[0])
+        nn = f32(np.sqrt(np.float64(f32(f32(f32(ux * ux) + f32(uy * uy)) + f32(uz * uz)))))
+        p.anis_axis[0], p.anis_axis[1], p.anis_axis[2] = f32(ux / nn), f32(uy / nn), f32(uz / nn)
+    p.solver = SOLVERS[solver]
+    dti = f32(f32(dt) / u["time"])
+    p.dt = dti if dti != 0 else f32(1e-4)
+    p.max_error = maxerror
+    p.unit_time = u["time"]
+    p.exch_type = exch_type
+    p.faithful = faithful
+    p.accuracy = 8
+    return p
+
+
+class Solver:
+    """The fused solver (mmx_solver_*), state resident on the device."""
+
+    def __init__(self, params):
+        self.params = params
+        self.h = ctypes.c_void_p()
+        _check(lib().mmx_solver_create(ctypes.byref(params), ctypes.byref(self.h)))
+        self.N = (params.size[0], params.size[1], params.size[2])
+        self.n = self.N[0] * self.N[1] * self.N[2]
+
+    def close(self):
+        if self.h:
+            lib().mmx_solver_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_m(self, m, stream=None):
+        a = np.ascontiguousarray(m, dtype=np.float32)
+        assert a.size == 3 * self.n
+        _check(lib().mmx_solver_set_m(self.h, a.ctypes.data, 1, stream))
+
+    def set_m_device(self, ptr, stream=None):
+        _check(lib().mmx_solver_set_m(self.h, ptr, 0, stream))
+
+    def get_m(self, stream=None):
+        out = np.empty((3,) + self.N, dtype=np.float32)
+        _check(lib().mmx_solver_get_m(self.h, out.ctypes.data, 1, stream))
+        return out
+
+    def normalize(self, stream=None):
+        _check(lib().mmx_solver_normalize(self.h, stream))
+
+    def step(self, n=1, stream=None):
+        _check(lib().mmx_solver_step(self.h, n, stream))
+
+    def field(self, m_ptr, h_ptr, stream=None):
+        _check(lib().mmx_solver_field(self.h, m_ptr, h_ptr, stream))
+
+    def state(self):
+        t, dt, tq, er, st = ctypes.c_double(), ctypes.c_float(), ctypes.c_float(), ctypes.c_float(), ctypes.c_longlong()
+        _check(lib().mmx_solver_state(self.h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(tq), ctypes.byref(er),
+                                      ctypes.byref(st)))
+        return dict(time=t.value, dt=dt.value, torque=tq.value, error=er.value, steps=st.value)
+
+    def m_device(self):
+        return lib().mmx_solver_m_device(self.h)
+
+    def use_graph(self, on=True):
+        _check(lib().mmx_solver_use_graph(self.h, 1 if on else 0))
+
+    def profile(self, on=True):
+        _check(lib().mmx_solver_profile(self.h, 1 if on else 0))
+
+    def pass_times(self):
+        names = (ctypes.c_char * 32 * 32)()
+        ms = (ctypes.c_double * 32)()
+        la = (ctypes.c_longlong * 32)()
+        n = ctypes.c_int()
+        _check(lib().mmx_solver_pass_times(self.h, 32, names, ms, la, ctypes.byref(n)))
+        return {names[i].value.decode(): (ms[i], la[i]) for i in range(n.value)}
+
+
+def face_kernel6_device(P, periodic, cellsize, exch6=True, accuracy=8, out_ptr=None, stream=None):
+    """Runs mmx_face_kernel6 into a device buffer of 6*P0*P1*P2 floats."""
+    Pa = (ctypes.c_int * 3)(*P)
+    pa = (ctypes.c_int * 3)(*periodic)
+    ca = (ctypes.c_float * 3)(*[float(c) for c in cellsize])
+    _check(lib().mmx_face_kernel6(Pa, pa, ca, accuracy, 1 if exch6 else 0, out_ptr, stream))
+
+
+def driver_config(grid, cell, msat, aexch, alpha, bext=(0, 0, 0), solver="heun", dt=0.0, maxerror=0.0, anis=0,
+                  k1=0.0, axis=(0, 0, 1), periodic=(0, 0, 0), faithful=1, mindm=0.0, maxdm=0.0, mindt=0.0,
+                  maxdt=0.0):
+    c = DriverConfig()
+    c.grid[:] = list(grid)
+    c.cell[:] = list(cell)
+    c.periodic[:] = list(periodic)
+    c.msat, c.aexch, c.alpha = msat, aexch, alpha
+    c.bext[:] = list(bext)
+    c.anis_type, c.k1 = anis, k1
+    c.anis_axis[:] = list(axis)
+    c.solver = SOLVERS[solver]
+    c.dt, c.maxerror = dt, maxerror
+    c.mindm, c.maxdm, c.mindt, c.maxdt = mindm, maxdm, mindt, maxdt
+    c.faithful = faithful
+    return c
+
+
+class DriverSim:
+    """The Go-driver restatement (libmmxdriver.so) over a libgpukern
+    implementation given by path (the B200 engine by default)."""
+
+    def __init__(self, cfg, m_internal, k6, libpath=LIB_PATH):
+        D = driver()
+        self.L = D.mmxd_open(libpath.encode())
+        if not self.L:
+            raise MmxError("mmxd_open(%s): %s" % (libpath, D.mmxd_last_error().decode()))
+        self.m0 = np.ascontiguousarray(m_internal, dtype=np.float32)
+        self.k6 = np.ascontiguousarray(k6, dtype=np.float32)
+        self.h = D.mmxd_new(self.L, ctypes.byref(cfg), self.m0.ctypes.data, self.k6.ctypes.data)
+        if not self.h:
+            raise MmxError("mmxd_new: %s" % D.mmxd_last_error().decode())
+        N = (ctypes.c_int * 3)()
+        P = (ctypes.c_int * 3)()
+        D.mmxd_sizes(self.h, N, P)
+        self.N, self.P = tuple(N), tuple(P)
+
+    def close(self):
+        D = driver()
+        if getattr(self, "h", None):
+            D.mmxd_free(self.h)
+            self.h = None
+        if getattr(self, "L", None):
+            D.mmxd_close(self.L)
+            self.L = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def steps(self, n):
+        rc = driver().mmxd_steps(self.h, n)
+        if rc:
+            raise MmxError(driver().mmxd_last_error().decode())
+
+    def run(self, seconds):
+        rc = driver().mmxd_run(self.h, seconds)
+        if rc:
+            raise MmxError(driver().mmxd_last_error().decode())
+
+    def m(self):
+        out = np.empty((3,) + self.N, dtype=np.float32)
+        driver().mmxd_get_m(self.h, out.ctypes.data)
+        return out
+
+    def set_m(self, m):
+        a = np.ascontiguousarray(m, dtype=np.float32)
+        driver().mmxd_set_m(self.h, a.ctypes.data)
+
+    def heff(self, m):
+        a = np.ascontiguousarray(m, dtype=np.float32)
+        out = np.empty_like(a)
+        driver().mmxd_heff(self.h, a.ctypes.data, out.ctypes.data)
+        return out
+
+    def avg_m(self):
+        out = np.zeros(3, np.float32)
+        driver().mmxd_avg_m(self.h, out.ctypes.data)
+        return out
+
+    def time(self):
+        return driver().mmxd_time(self.h)
+
+    def dt(self):
+        return driver().mmxd_dt(self.h)
+
+    def torque(self):
+        return driver().mmxd_torque(self.h)

@@ -1,0 +1,1093 @@
+// Drop-in libgpukern C ABI (see include/gpukern.h).
+//
+// Each entry point keeps the reference's contract: synchronous, raw float*
+// device arrays, host scalars/arrays where the reference takes them, abort
+// with a message on any CUDA error or bad argument.  The arithmetic of the
+// element-wise entry points follows the reference's operation order with
+// one IEEE rounding per operation (no contraction); normalisation uses a
+// correctly rounded 1/sqrt instead of the fast-math rsqrtf.
+//
+// Documented departures from the reference (all fixes of reference bugs,
+// none on values the Go driver consumes):
+//  * gpu_copy_unpad copies only the D0 destination planes (the reference
+//    loops over the S0 source planes and writes past the destination,
+//    gpu_zeropad.cu:97-107);
+//  * gpuFFT3dPlan_inverse leaves its spectrum input partly overwritten by
+//    intermediate results instead of holding the full C2R output (the Go
+//    driver never reads it, conv.go:96-99);
+//  * cubic anisotropy with a field mask reads Hext[X..Z], not Hext[X*N]
+//    (gpu_local_contr3.cu:217);
+//  * gpu_add_lin_anisotropy performs its computation (the reference's host
+//    function is empty, gpu_anis.cu:44-50);
+//  * gpu_directionial_diff indexes from the array base once (the reference
+//    offsets the pointer and the index, gpu_spintorque.cu:254-258);
+//  * gpu_linear_combination_many reads result[i] only for i < N
+//    (gpu_linalg.cu:103-112 reads before the bounds check);
+//  * gpu_gaussian_noise uses a counter-based Philox generator of its own
+//    (reference: cuRAND default generator, gpu_temperature.cu:34-41).
+#include <assert.h>
+#include <math.h>
+#include <string.h>
+
+#include "fft_passes.cuh"
+#include "llg_ops.cuh"
+#include "mmx_common.cuh"
+#include "../../include/gpukern.h"
+
+#define ABI_ASSERT(cond, msg) MMX_ABORT_ON(!(cond), "%s (%s)", msg, #cond)
+
+static const int EW_BLOCK = 256;
+static int ew_grid(int64_t n) {
+  int64_t b = (n + EW_BLOCK - 1) / EW_BLOCK;
+  int64_t cap = (int64_t)mmx_sm_count() * 16;
+  if (b < 1) b = 1;
+  return (int)(b < cap ? b : cap);
+}
+#define GRID_STRIDE(i, n) \
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+// Every exported function below is declared extern "C" in gpukern.h and so
+// keeps C linkage here.
+
+// ---------------------------------------------------------------------
+// init / conf / properties / streams
+// ---------------------------------------------------------------------
+static int g_maxthreads = 0;
+static cudaDeviceProp g_prop;
+static int g_prop_dev = -1;
+
+void* gpu_getproperties(void) {
+  int dev = 0;
+  GK_CHECK(cudaGetDevice(&dev));
+  if (g_prop_dev != dev) {
+    GK_CHECK(cudaGetDeviceProperties(&g_prop, dev));
+    g_prop_dev = dev;
+  }
+  return &g_prop;
+}
+
+void gpu_print_properties(FILE* out) {
+  cudaDeviceProp* p = (cudaDeviceProp*)gpu_getproperties();
+  fprintf(out, "     Device number: %d\n", g_prop_dev);
+  fprintf(out, "       Device name: %s\n", p->name);
+  fprintf(out, "     Global Memory: %zu MB\n", (size_t)(p->totalGlobalMem / (1024 * 1024)));
+  fprintf(out, "     Shared Memory: %zu kB/block\n", (size_t)(p->sharedMemPerBlock / 1024));
+  fprintf(out, "   Const.  Memory: %zu B\n", (size_t)p->totalConstMem);
+  fprintf(out, "         Registers: %d per block\n", p->regsPerBlock);
+  fprintf(out, "         Warp size: %d threads\n", p->warpSize);
+  fprintf(out, "  Max thread block: %d threads\n", p->maxThreadsPerBlock);
+  fprintf(out, " Compute capability: %d.%d\n", p->major, p->minor);
+  fprintf(out, "   Multiprocessors: %d\n", p->multiProcessorCount);
+}
+
+void gpu_print_properties_stdout(void) { gpu_print_properties(stdout); }
+
+int gpu_maxthreads(void) {
+  if (g_maxthreads <= 0) g_maxthreads = ((cudaDeviceProp*)gpu_getproperties())->maxThreadsPerBlock;
+  return g_maxthreads;
+}
+void gpu_setmaxthreads(int max) { g_maxthreads = max; }
+
+// gpu_init.cu:24-27: only the threads-per-block setting is taken
+void gpu_init(int threads, int options) {
+  (void)options;
+  gpu_setmaxthreads(threads);
+}
+void gpu_set_device(int devid) { GK_CHECK(cudaSetDevice(devid)); }
+
+void check3dconf(dim3 g, dim3 b) {
+  cudaDeviceProp* p = (cudaDeviceProp*)gpu_getproperties();
+  ABI_ASSERT(g.x > 0 && g.y > 0 && g.z > 0 && b.x > 0 && b.y > 0 && b.z > 0, "check3dconf");
+  ABI_ASSERT((int)b.x <= p->maxThreadsDim[0] && (int)b.y <= p->maxThreadsDim[1] && (int)b.z <= p->maxThreadsDim[2],
+             "check3dconf");
+  ABI_ASSERT((int)g.x <= p->maxGridSize[0] && (int)g.y <= p->maxGridSize[1] && (int)g.z <= p->maxGridSize[2],
+             "check3dconf");
+  ABI_ASSERT((int)(b.x * b.y * b.z) <= p->maxThreadsPerBlock, "check3dconf");
+}
+void check1dconf(int g, int b) {
+  ABI_ASSERT(g > 0 && b > 0 && b <= ((cudaDeviceProp*)gpu_getproperties())->maxThreadsPerBlock, "check1dconf");
+}
+// gpu_conf.cu:68-97
+void make1dconf(int N, dim3* gridSize, dim3* blockSize) {
+  cudaDeviceProp* p = (cudaDeviceProp*)gpu_getproperties();
+  int mb = gpu_maxthreads();
+  int mg = p->maxGridSize[0];
+  *blockSize = dim3(mb, 1, 1);
+  int N2 = (N - 1) / mb + 1;
+  int NX = (N2 - 1) / mg + 1;
+  int NY = (N2 - 1) / NX + 1;
+  *gridSize = dim3(NX, NY, 1);
+  check3dconf(*gridSize, *blockSize);
+}
+
+#define MAXGPUSTREAMS 32
+static cudaStream_t g_streams[MAXGPUSTREAMS];
+static int g_stream_init = 0, g_stream_cur = 0;
+void gpu_init_stream(void) {
+  for (int i = 0; i < MAXGPUSTREAMS; i++) GK_CHECK(cudaStreamCreate(&g_streams[i]));
+  g_stream_init = 1;
+  g_stream_cur = 0;
+}
+cudaStream_t gpu_getstream(void) {
+  if (!g_stream_init) gpu_init_stream();
+  cudaStream_t s = g_streams[g_stream_cur];
+  g_stream_cur = (g_stream_cur + 1) % MAXGPUSTREAMS;
+  return s;
+}
+
+// ---------------------------------------------------------------------
+// memory
+// ---------------------------------------------------------------------
+static unsigned long long g_usedmem = 0;
+static int g_stride_cache = -1;
+
+__global__ void k_zero(float* a, int64_t n) {
+  GRID_STRIDE(i, n) a[i] = 0.f;
+}
+
+void gpu_zero(float* data, int n) {
+  ABI_ASSERT(n >= 0, "gpu_zero");
+  if (n == 0) return;
+  k_zero<<<ew_grid(n), EW_BLOCK>>>(data, n);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_zero_async(float* data, int n) { GK_CHECK(cudaMemsetAsync(data, 0, sizeof(float) * (size_t)n, 0)); }
+
+float* new_gpu_array(int size) {
+  ABI_ASSERT(size > 0, "new_gpu_array: size must be > 0");
+  float* a = nullptr;
+  GK_CHECK(cudaMalloc((void**)&a, sizeof(float) * (size_t)size));
+  g_usedmem += sizeof(float) * (unsigned long long)size;
+  gpu_zero(a, size);
+  return a;
+}
+void free_gpu_array(float* p) { GK_CHECK(cudaFree(p)); }
+unsigned long long int gpu_usedmem(void) { return g_usedmem; }
+
+float* new_ram_array(int size) {
+  ABI_ASSERT(size > 0, "new_ram_array");
+  float* a = (float*)calloc((size_t)size, sizeof(float));
+  MMX_ABORT_ON(!a, "could not allocate %d floats in main memory", size);
+  return a;
+}
+
+int gpu_stride_float(void) {
+  if (g_stride_cache == -1) {
+    float* p = nullptr;
+    size_t pitch = 0;
+    GK_CHECK(cudaMallocPitch((void**)&p, &pitch, sizeof(float), 1));
+    GK_CHECK(cudaFree(p));
+    g_stride_cache = (int)(pitch / sizeof(float));
+  }
+  return g_stride_cache;
+}
+void gpu_override_stride(int nFloats) {
+  ABI_ASSERT(nFloats > -2, "gpu_override_stride");
+  g_stride_cache = nFloats;
+}
+
+void memcpy_to_gpu(float* src, float* dst, int n) {
+  ABI_ASSERT(n > 0, "memcpy_to_gpu");
+  GK_CHECK(cudaMemcpy(dst, src, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice));
+  GK_SYNC();
+}
+void memcpy_from_gpu(float* src, float* dst, int n) {
+  ABI_ASSERT(n > 0, "memcpy_from_gpu");
+  GK_CHECK(cudaMemcpy(dst, src, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost));
+  GK_SYNC();
+}
+void memcpy_on_gpu(float* src, float* dst, int n) {
+  ABI_ASSERT(n > 0, "memcpy_on_gpu");
+  GK_CHECK(cudaMemcpy(dst, src, sizeof(float) * (size_t)n, cudaMemcpyDeviceToDevice));
+  GK_SYNC();
+}
+void memcpy_on_gpu_async(float* src, float* dst, int n) {
+  ABI_ASSERT(n > 0, "memcpy_on_gpu_async");
+  GK_CHECK(cudaMemcpy(dst, src, sizeof(float) * (size_t)n, cudaMemcpyDeviceToDevice));
+}
+void memcpy_gpu_dir(float* src, float* dst, int n, int dir) {
+  if (dir == DIR_TO) memcpy_to_gpu(src, dst, n);
+  else if (dir == DIR_ON) memcpy_on_gpu(src, dst, n);
+  else if (dir == DIR_FROM) memcpy_from_gpu(src, dst, n);
+  else MMX_ABORT_ON(1, "illegal memcpy direction: %d", dir);
+}
+float gpu_array_get(float* p, int index) {
+  float r = 0;
+  memcpy_from_gpu(p + index, &r, 1);
+  return r;
+}
+void gpu_array_set(float* p, int index, float value) { memcpy_to_gpu(&value, p + index, 1); }
+
+static float g_host_probe[1];
+static float* g_dev_probe = nullptr;
+void assertHost(float* pointer) { g_host_probe[0] = pointer[0]; }
+void assertDevice(float* pointer) {
+  if (!g_dev_probe) g_dev_probe = new_gpu_array(1);
+  memcpy_on_gpu(pointer, g_dev_probe, 1);
+}
+
+// ---------------------------------------------------------------------
+// vector algebra (gpu_linalg.cu:21-140)
+// ---------------------------------------------------------------------
+__global__ void k_add(float* a, const float* b, int64_t n) { GRID_STRIDE(i, n) a[i] = FA(a[i], b[i]); }
+__global__ void k_madd(float* a, float c, const float* b, int64_t n) { GRID_STRIDE(i, n) a[i] = FA(a[i], FM(c, b[i])); }
+__global__ void k_madd2(float* a, const float* b, const float* c, int64_t n) {
+  GRID_STRIDE(i, n) a[i] = FA(a[i], FM(b[i], c[i]));
+}
+__global__ void k_add_constant(float* a, float c, int64_t n) { GRID_STRIDE(i, n) a[i] = FA(a[i], c); }
+__global__ void k_lincomb(float* a, const float* b, float wa, float wb, int64_t n) {
+  GRID_STRIDE(i, n) a[i] = FA(FM(wa, a[i]), FM(wb, b[i]));
+}
+__global__ void k_lincomb_many(float* r, float* const* v, const float* w, int nv, int64_t n) {
+  GRID_STRIDE(i, n) {
+    float acc = r[i];
+    for (int j = 0; j < nv; j++) acc = FA(acc, FM(w[j], v[j][i]));
+    r[i] = acc;
+  }
+}
+__global__ void k_scale_dot(float* r, const float* a, const float* b, float s, int64_t n) {
+  GRID_STRIDE(i, n) r[i] = FM(s, FA(FA(FM(a[i], b[i]), FM(a[n + i], b[n + i])), FM(a[2 * n + i], b[2 * n + i])));
+}
+
+void gpu_add(float* a, float* b, int N) {
+  k_add<<<ew_grid(N), EW_BLOCK>>>(a, b, N);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_madd(float* a, float cnst, float* b, int N) {
+  k_madd<<<ew_grid(N), EW_BLOCK>>>(a, cnst, b, N);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_madd2(float* a, float* b, float* c, int N) {
+  k_madd2<<<ew_grid(N), EW_BLOCK>>>(a, b, c, N);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_add_constant(float* a, float cnst, int N) {
+  k_add_constant<<<ew_grid(N), EW_BLOCK>>>(a, cnst, N);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_linear_combination(float* a, float* b, float wA, float wB, int N) {
+  k_lincomb<<<ew_grid(N), EW_BLOCK>>>(a, b, wA, wB, N);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+// vectors and weights are device arrays in the reference kernel
+// (gpu_linalg.cu:103-121 dereferences both on the device)
+void gpu_linear_combination_many(float* result, float** vectors, float* weights, int NVectors, int NElem) {
+  k_lincomb_many<<<ew_grid(NElem), EW_BLOCK>>>(result, vectors, weights, NVectors, NElem);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_scale_dot_product(float* result, float* v1, float* v2, float a, int N) {
+  k_scale_dot<<<ew_grid(N), EW_BLOCK>>>(result, v1, v2, a, N);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+
+// ---------------------------------------------------------------------
+// normalise, torque
+// ---------------------------------------------------------------------
+__global__ void k_normalize_uniform(float* m, int64_t n) {
+  GRID_STRIDE(i, n) {
+    float x = m[i], y = m[n + i], z = m[2 * n + i];
+    llg_normalize(x, y, z);
+    m[i] = x;
+    m[n + i] = y;
+    m[2 * n + i] = z;
+  }
+}
+// gpu_normalize.cu:47-58: norm * map, zero where the map is zero
+__global__ void k_normalize_map(float* m, const float* map, int64_t n) {
+  GRID_STRIDE(i, n) {
+    float x = m[i], y = m[n + i], z = m[2 * n + i];
+    float s = FA(FA(FM(x, x), FM(y, y)), FM(z, z));
+    float nrm = FM(__fdiv_rn(1.f, __fsqrt_rn(s)), map[i]);
+    if (map[i] == 0.f) nrm = 0.f;
+    m[i] = FM(x, nrm);
+    m[n + i] = FM(y, nrm);
+    m[2 * n + i] = FM(z, nrm);
+  }
+}
+__global__ void k_delta_m(const float* m, float* h, float alpha_mul, const float* alpha_map, float dtg, int64_t n) {
+  GRID_STRIDE(i, n) {
+    float alpha = alpha_map ? FM(alpha_mul, alpha_map[i]) : alpha_mul;
+    float hx = h[i], hy = h[n + i], hz = h[2 * n + i];
+    llg_delta_m(m[i], m[n + i], m[2 * n + i], hx, hy, hz, alpha, dtg);
+    h[i] = hx;
+    h[n + i] = hy;
+    h[2 * n + i] = hz;
+  }
+}
+
+void gpu_normalize_uniform(float* m, int N) {
+  k_normalize_uniform<<<ew_grid(N), EW_BLOCK>>>(m, N);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_normalize_map(float* m, float* map, int N) {
+  k_normalize_map<<<ew_grid(N), EW_BLOCK>>>(m, map, N);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_deltaM(float* m, float* h, float alpha_mul, float* alpha_map, float dt_gilb, int N) {
+  k_delta_m<<<ew_grid(N), EW_BLOCK>>>(m, h, alpha_mul, alpha_map, dt_gilb, N);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+
+// ---------------------------------------------------------------------
+// local fields (gpu_local_contr3.cu)
+// ---------------------------------------------------------------------
+struct LF {
+  float hx, hy, hz;
+  int type;
+  float K0, K1;
+  float U[9];
+};
+
+__device__ __forceinline__ void cubic_terms(const LF& p, float mx, float my, float mz, float& c0, float& c1,
+                                            float& c2, float* dd) {
+  const float* U = p.U;
+  float a0 = FA(FA(FM(mx, U[0]), FM(my, U[1])), FM(mz, U[2]));
+  float a1 = FA(FA(FM(mx, U[3]), FM(my, U[4])), FM(mz, U[5]));
+  float a2 = FA(FA(FM(mx, U[6]), FM(my, U[7])), FM(mz, U[8]));
+  float a00 = FM(a0, a0), a11 = FM(a1, a1), a22 = FM(a2, a2);
+  float d0 = FA(FM(FM(p.K0, FA(a11, a22)), a0), FM(FM(FM(p.K1, a0), a11), a22));
+  float d1 = FA(FM(FM(p.K0, FA(a00, a22)), a1), FM(FM(FM(p.K1, a00), a1), a22));
+  float d2 = FA(FM(FM(p.K0, FA(a00, a11)), a2), FM(FM(FM(p.K1, a00), a11), a2));
+  dd[0] = d0;
+  dd[1] = d1;
+  dd[2] = d2;
+  c0 = FA(FA(FM(d0, U[0]), FM(d1, U[3])), FM(d2, U[6]));
+  c1 = FA(FA(FM(d0, U[1]), FM(d1, U[4])), FM(d2, U[7]));
+  c2 = FA(FA(FM(d0, U[2]), FM(d1, U[5])), FM(d2, U[8]));
+}
+
+template <bool PHI>
+__global__ void k_local_fields(const float* m, float* h, float* phi, int64_t n, LF p, const float* hmap) {
+  GRID_STRIDE(i, n) {
+    float mx = m[i], my = m[n + i], mz = m[2 * n + i];
+    float ex = p.hx, ey = p.hy, ez = p.hz;
+    if (hmap) {
+      ex = FM(ex, hmap[i]);
+      ey = FM(ey, hmap[n + i]);
+      ez = FM(ez, hmap[2 * n + i]);
+    }
+    float hx = h[i], hy = h[n + i], hz = h[2 * n + i];
+    float dphi = 0.f;
+    if (p.type == 1) {
+      float mu = FA(FA(FM(mx, p.U[0]), FM(my, p.U[1])), FM(mz, p.U[2]));
+      float km = FM(p.K0, mu);
+      hx = FA(hx, FA(ex, FM(km, p.U[0])));
+      hy = FA(hy, FA(ey, FM(km, p.U[1])));
+      hz = FA(hz, FA(ez, FM(km, p.U[2])));
+      if (PHI) {
+        float mh = FA(FA(FM(mx, ex), FM(my, ey)), FM(mz, ez));
+        float an = FM(FM(FM(0.5f, p.K0), mu), mu);
+        dphi = FA(mh, an);
+      }
+    } else if (p.type == 2) {
+      float c0, c1, c2, d[3];
+      cubic_terms(p, mx, my, mz, c0, c1, c2, d);
+      if (PHI) {  // gpu_local_contr3.cu:296-303
+        hx = FA(hx, FS(ex, c0));
+        hy = FA(hy, FS(ey, c1));
+        hz = FA(hz, FS(ez, c2));
+      } else {    // gpu_local_contr3.cu:85-87
+        hx = FA(hx, FS(FS(FS(ex, FM(d[0], p.U[0])), FM(d[1], p.U[3])), FM(d[2], p.U[6])));
+        hy = FA(hy, FS(FS(FS(ey, FM(d[0], p.U[1])), FM(d[1], p.U[4])), FM(d[2], p.U[7])));
+        hz = FA(hz, FS(FS(FS(ez, FM(d[0], p.U[2])), FM(d[1], p.U[5])), FM(d[2], p.U[8])));
+      }
+      if (PHI) {
+        float mh = FA(FA(FM(mx, ex), FM(my, ey)), FM(mz, ez));
+        float mc = FA(FA(FM(mx, c0), FM(my, c1)), FM(mz, c2));
+        dphi = FS(mh, FM(0.25f, mc));
+      }
+    } else {
+      hx = FA(hx, ex);
+      hy = FA(hy, ey);
+      hz = FA(hz, ez);
+      if (PHI) dphi = FA(FA(FM(mx, ex), FM(my, ey)), FM(mz, ez));
+    }
+    h[i] = hx;
+    h[n + i] = hy;
+    h[2 * n + i] = hz;
+    if (PHI) phi[i] = FS(phi[i], dphi);
+  }
+}
+
+static LF make_lf(float* Hext, int anisType, float* anisK, float* anisAxes) {
+  LF p;
+  memset(&p, 0, sizeof(p));
+  p.hx = Hext[0];
+  p.hy = Hext[1];
+  p.hz = Hext[2];
+  p.type = anisType;
+  MMX_ABORT_ON(anisType < 0 || anisType > 2, "unknown anisotropy type %d", anisType);
+  if (anisType == 1) {
+    p.K0 = anisK[0];
+    for (int d = 0; d < 3; d++) p.U[d] = anisAxes[d];
+  } else if (anisType == 2) {
+    p.K0 = anisK[0];
+    p.K1 = anisK[1];
+    for (int d = 0; d < 9; d++) p.U[d] = anisAxes[d];
+  }
+  return p;
+}
+
+void gpu_add_local_fields(float* m, float* h, int N, float* Hext, float* hmap, int anisType, float* anisK,
+                          float* anisAxes) {
+  LF p = make_lf(Hext, anisType, anisK, anisAxes);
+  k_local_fields<false><<<ew_grid(N), EW_BLOCK>>>(m, h, nullptr, N, p, hmap);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_add_local_fields_H_and_phi(float* m, float* h, float* phi, int N, float* Hext, float* hmap, int anisType,
+                                    float* anisK, float* anisAxes) {
+  LF p = make_lf(Hext, anisType, anisK, anisAxes);
+  k_local_fields<true><<<ew_grid(N), EW_BLOCK>>>(m, h, phi, N, p, hmap);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+
+// ---------------------------------------------------------------------
+// kernel multiplications (gpu_kernmul.cu)
+// ---------------------------------------------------------------------
+__global__ void k_kmul6(float2* mx, float2* my, float2* mz, const float* kxx, const float* kyy, const float* kzz,
+                        const float* kyz, const float* kxz, const float* kxy, int64_t n) {
+  GRID_STRIDE(i, n) {
+    float2 a = mx[i], b = my[i], c = mz[i];
+    float Kxx = kxx[i], Kyy = kyy[i], Kzz = kzz[i], Kyz = kyz[i], Kxz = kxz[i], Kxy = kxy[i];
+    mx[i] = make_float2(FA(FA(FM(a.x, Kxx), FM(b.x, Kxy)), FM(c.x, Kxz)), FA(FA(FM(a.y, Kxx), FM(b.y, Kxy)), FM(c.y, Kxz)));
+    my[i] = make_float2(FA(FA(FM(a.x, Kxy), FM(b.x, Kyy)), FM(c.x, Kyz)), FA(FA(FM(a.y, Kxy), FM(b.y, Kyy)), FM(c.y, Kyz)));
+    mz[i] = make_float2(FA(FA(FM(a.x, Kxz), FM(b.x, Kyz)), FM(c.x, Kzz)), FA(FA(FM(a.y, Kxz), FM(b.y, Kyz)), FM(c.y, Kzz)));
+  }
+}
+__global__ void k_kmul4(float2* mx, float2* my, float2* mz, const float* kxx, const float* kyy, const float* kzz,
+                        const float* kyz, int64_t n) {
+  GRID_STRIDE(i, n) {
+    float2 a = mx[i], b = my[i], c = mz[i];
+    float Kxx = kxx[i], Kyy = kyy[i], Kzz = kzz[i], Kyz = kyz[i];
+    mx[i] = make_float2(FM(a.x, Kxx), FM(a.y, Kxx));
+    my[i] = make_float2(FA(FM(b.x, Kyy), FM(c.x, Kyz)), FA(FM(b.y, Kyy), FM(c.y, Kyz)));
+    mz[i] = make_float2(FA(FM(b.x, Kyz), FM(c.x, Kzz)), FA(FM(b.y, Kyz), FM(c.y, Kzz)));
+  }
+}
+__global__ void k_kmul3(float2* my, float2* mz, const float* kyy, const float* kzz, const float* kyz, int64_t n) {
+  GRID_STRIDE(i, n) {
+    float2 b = my[i], c = mz[i];
+    float Kyy = kyy[i], Kzz = kzz[i], Kyz = kyz[i];
+    my[i] = make_float2(FA(FM(b.x, Kyy), FM(c.x, Kyz)), FA(FM(b.y, Kyy), FM(c.y, Kyz)));
+    mz[i] = make_float2(FA(FM(b.x, Kyz), FM(c.x, Kzz)), FA(FM(b.y, Kyz), FM(c.y, Kzz)));
+  }
+}
+// mode 0: 3D, 1: 3D with Kx = 0 (Nx1), 2: 2D (gpu_kernmul.cu:180-330)
+__global__ void k_biot(float2* jx, float2* jy, float2* jz, const float* kx, const float* ky, const float* kz, int mode,
+                       int64_t n) {
+  GRID_STRIDE(i, n) {
+    float2 a = jx[i], b = jy[i], c = jz[i];
+    float Kx = mode == 0 ? kx[i] : 0.f, Ky = ky[i], Kz = kz[i];
+    if (mode == 2) {
+      jy[i] = make_float2(FM(-a.x, Kz), FM(-a.y, Kz));
+      jz[i] = make_float2(FM(a.x, Ky), FM(a.y, Ky));
+      continue;
+    }
+    jx[i] = make_float2(FS(FM(b.x, Kz), FM(c.x, Ky)), FS(FM(b.y, Kz), FM(c.y, Ky)));
+    if (mode == 0) {
+      jy[i] = make_float2(FA(FM(-a.x, Kz), FM(c.x, Kx)), FA(FM(-a.y, Kz), FM(c.y, Kx)));
+      jz[i] = make_float2(FS(FM(a.x, Ky), FM(b.x, Kx)), FS(FM(a.y, Ky), FM(b.y, Kx)));
+    } else {
+      jy[i] = make_float2(FM(-a.x, Kz), FM(-a.y, Kz));
+      jz[i] = make_float2(FM(a.x, Ky), FM(a.y, Ky));
+    }
+  }
+}
+
+void gpu_kernelmul6(float* fftMx, float* fftMy, float* fftMz, float* fftKxx, float* fftKyy, float* fftKzz,
+                    float* fftKyz, float* fftKxz, float* fftKxy, int nRealNumbers) {
+  ABI_ASSERT(nRealNumbers > 0 && nRealNumbers % 2 == 0, "gpu_kernelmul6");
+  int64_t n = nRealNumbers / 2;
+  k_kmul6<<<ew_grid(n), EW_BLOCK>>>((float2*)fftMx, (float2*)fftMy, (float2*)fftMz, fftKxx, fftKyy, fftKzz, fftKyz,
+                                    fftKxz, fftKxy, n);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_kernelmul4(float* fftMx, float* fftMy, float* fftMz, float* fftKxx, float* fftKyy, float* fftKzz,
+                    float* fftKyz, int nRealNumbers) {
+  ABI_ASSERT(nRealNumbers > 0 && nRealNumbers % 2 == 0, "gpu_kernelmul4");
+  int64_t n = nRealNumbers / 2;
+  k_kmul4<<<ew_grid(n), EW_BLOCK>>>((float2*)fftMx, (float2*)fftMy, (float2*)fftMz, fftKxx, fftKyy, fftKzz, fftKyz, n);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_kernelmul3(float* fftMy, float* fftMz, float* fftKyy, float* fftKzz, float* fftKyz, int nRealNumbers) {
+  ABI_ASSERT(nRealNumbers > 0 && nRealNumbers % 2 == 0, "gpu_kernelmul3");
+  int64_t n = nRealNumbers / 2;
+  k_kmul3<<<ew_grid(n), EW_BLOCK>>>((float2*)fftMy, (float2*)fftMz, fftKyy, fftKzz, fftKyz, n);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_kernelmul_biot_savart3D(float* fftJx, float* fftJy, float* fftJz, float* fftKx, float* fftKy, float* fftKz,
+                                 int nRealNumbers) {
+  ABI_ASSERT(nRealNumbers > 0 && nRealNumbers % 2 == 0, "gpu_kernelmul_biot_savart3D");
+  int64_t n = nRealNumbers / 2;
+  k_biot<<<ew_grid(n), EW_BLOCK>>>((float2*)fftJx, (float2*)fftJy, (float2*)fftJz, fftKx, fftKy, fftKz, 0, n);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_kernelmul_biot_savart3DNx1(float* fftJx, float* fftJy, float* fftJz, float* fftKy, float* fftKz,
+                                    int nRealNumbers) {
+  ABI_ASSERT(nRealNumbers > 0 && nRealNumbers % 2 == 0, "gpu_kernelmul_biot_savart3DNx1");
+  int64_t n = nRealNumbers / 2;
+  k_biot<<<ew_grid(n), EW_BLOCK>>>((float2*)fftJx, (float2*)fftJy, (float2*)fftJz, nullptr, fftKy, fftKz, 1, n);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_kernelmul_biot_savart2D(float* fftJx, float* fftJy, float* fftJz, float* fftKy, float* fftKz,
+                                 int nRealNumbers) {
+  ABI_ASSERT(nRealNumbers > 0 && nRealNumbers % 2 == 0, "gpu_kernelmul_biot_savart2D");
+  int64_t n = nRealNumbers / 2;
+  k_biot<<<ew_grid(n), EW_BLOCK>>>((float2*)fftJx, (float2*)fftJy, (float2*)fftJz, nullptr, fftKy, fftKz, 2, n);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+
+// ---------------------------------------------------------------------
+// zero padding (gpu_zeropad.cu): one launch over all planes
+// ---------------------------------------------------------------------
+__global__ void k_copy_box(const float* src, float* dst, int n0, int n1, int n2, int S1, int S2, int D1, int D2) {
+  int64_t total = (int64_t)n0 * n1 * n2;
+  GRID_STRIDE(e, total) {
+    int k = (int)(e % n2);
+    int j = (int)((e / n2) % n1);
+    int i = (int)(e / ((int64_t)n1 * n2));
+    dst[((int64_t)i * D1 + j) * D2 + k] = src[((int64_t)i * S1 + j) * S2 + k];
+  }
+}
+static void copy_box(const float* src, float* dst, int n0, int S1, int S2, int D1, int D2) {
+  int n1 = S1 < D1 ? S1 : D1, n2 = S2 < D2 ? S2 : D2;
+  int64_t total = (int64_t)n0 * n1 * n2;
+  if (total <= 0) return;
+  k_copy_box<<<ew_grid(total), EW_BLOCK>>>(src, dst, n0, n1, n2, S1, S2, D1, D2);
+  GK_LAUNCHED();
+}
+void gpu_copy_pad(float* source, float* dest, int S0, int S1, int S2, int D0, int D1, int D2) {
+  ABI_ASSERT(S0 <= D0 && S1 <= D1 && S2 <= D2, "gpu_copy_pad");
+  copy_box(source, dest, S0, S1, S2, D1, D2);
+  GK_SYNC();
+}
+void gpu_copy_unpad(float* source, float* dest, int S0, int S1, int S2, int D0, int D1, int D2) {
+  ABI_ASSERT(S0 >= D0 && S1 >= D1 && S2 >= D2, "gpu_copy_unpad");
+  copy_box(source, dest, D0, S1, S2, D1, D2);
+  GK_SYNC();
+}
+void gpu_copy_pad2D_async(float* source, float* dest, int S1, int S2, int D1, int D2) {
+  ABI_ASSERT(S1 <= D1 && S2 <= D2, "gpu_copy_pad2D");
+  copy_box(source, dest, 1, S1, S2, D1, D2);
+}
+void gpu_copy_pad2D(float* source, float* dest, int S1, int S2, int D1, int D2) {
+  gpu_copy_pad2D_async(source, dest, S1, S2, D1, D2);
+  GK_SYNC();
+}
+void gpu_copy_unpad2D_async(float* source, float* dest, int S1, int S2, int D1, int D2) {
+  ABI_ASSERT(S1 >= D1 && S2 >= D2, "gpu_copy_unpad2D");
+  copy_box(source, dest, 1, S1, S2, D1, D2);
+}
+void gpu_copy_unpad2D(float* source, float* dest, int S1, int S2, int D1, int D2) {
+  gpu_copy_unpad2D_async(source, dest, S1, S2, D1, D2);
+  GK_SYNC();
+}
+
+// ---------------------------------------------------------------------
+// FFT plan (gpu_fft0.cu:118-199) on the engine's zero-aware passes
+// ---------------------------------------------------------------------
+gpuFFT3dPlan* new_gpuFFT3dPlan_padded(int* size, int* paddedSize) {
+  ABI_ASSERT(paddedSize[0] > 0 && paddedSize[1] > 1 && paddedSize[2] > 1, "new_gpuFFT3dPlan_padded");
+  gpuFFT3dPlan* plan = (gpuFFT3dPlan*)calloc(1, sizeof(gpuFFT3dPlan));
+  plan->size = (int*)calloc(3, sizeof(int));
+  plan->paddedSize = (int*)calloc(3, sizeof(int));
+  for (int d = 0; d < 3; d++) {
+    plan->size[d] = size[d];
+    plan->paddedSize[d] = paddedSize[d];
+  }
+  plan->paddedN = paddedSize[0] * paddedSize[1] * paddedSize[2];
+  plan->paddedComplexN = paddedSize[0] * paddedSize[1] * (paddedSize[2] + 2);
+  BoxPlan* bp = new BoxPlan();
+  int rc = box_plan_init(bp, size, paddedSize);
+  MMX_ABORT_ON(rc != MMX_OK,
+               "unsupported FFT size %dx%dx%d padded to %dx%dx%d (padded Z must be even; every padded size a "
+               "product of 2,3,5,7 and <= 16384)",
+               size[0], size[1], size[2], paddedSize[0], paddedSize[1], paddedSize[2]);
+  plan->engine = bp;
+  return plan;
+}
+gpuFFT3dPlan* new_gpuFFT3dPlan(int* size) { return new_gpuFFT3dPlan_padded(size, size); }
+void delete_gpuFFT3dPlan(gpuFFT3dPlan* plan) {
+  if (!plan) return;
+  delete (BoxPlan*)plan->engine;
+  free(plan->size);
+  free(plan->paddedSize);
+  free(plan);
+}
+void gpuFFT3dPlan_forward(gpuFFT3dPlan* plan, float* input, float* output) {
+  GK_CHECK(box_forward((BoxPlan*)plan->engine, input, (float2*)output, 0));
+  GK_SYNC();
+}
+void gpuFFT3dPlan_inverse(gpuFFT3dPlan* plan, float* input, float* output) {
+  GK_CHECK(box_inverse((BoxPlan*)plan->engine, (float2*)input, output, 0));
+  GK_SYNC();
+}
+int gpuFFT3dPlan_normalization(gpuFFT3dPlan* plan) {
+  return plan->paddedSize[0] * plan->paddedSize[1] * plan->paddedSize[2];
+}
+
+// ---------------------------------------------------------------------
+// reductions (gpu_reduction.cu): single pass, warp shuffles, sums in
+// float64; partial kernels keep the reference's block partition
+// ---------------------------------------------------------------------
+__device__ __forceinline__ double red_op(int op, double a, double b) {
+  switch (op) {
+    case REDUCE_ADD:
+    case REDUCE_SUMABS: return a + b;
+    case REDUCE_MAX:
+    case REDUCE_MAXABS: return fmax(a, b);
+    default: return fmin(a, b);
+  }
+}
+__device__ __forceinline__ double red_load(int op, float v) {
+  return (op == REDUCE_MAXABS || op == REDUCE_SUMABS) ? (double)fabsf(v) : (double)v;
+}
+__device__ __forceinline__ double red_ident(int op) {
+  return op == REDUCE_MAX ? -INFINITY : op == REDUCE_MIN ? INFINITY : 0.0;
+}
+__device__ double block_reduce(int op, double v) {
+  __shared__ double sh[32];
+  for (int o = 16; o > 0; o >>= 1) v = red_op(op, v, __shfl_xor_sync(0xffffffffu, v, o));
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  int nw = (blockDim.x + 31) >> 5;
+  v = threadIdx.x < nw ? sh[threadIdx.x] : red_ident(op);
+  if (w == 0)
+    for (int o = 16; o > 0; o >>= 1) v = red_op(op, v, __shfl_xor_sync(0xffffffffu, v, o));
+  __syncthreads();
+  return v;
+}
+// partial b covers {i : (i mod chunk*blocks) in [b*chunk, (b+1)*chunk)}
+__global__ void k_partial(int op, const float* in, float* out, int64_t n, int64_t chunk, int blocks) {
+  double v = red_ident(op);
+  int64_t stride = chunk * blocks;
+  for (int64_t base = (int64_t)blockIdx.x * chunk; base < n; base += stride)
+    for (int64_t i = base + threadIdx.x; i < base + chunk && i < n; i += blockDim.x) v = red_op(op, v, red_load(op, in[i]));
+  v = block_reduce(op, v);
+  if (threadIdx.x == 0) out[blockIdx.x] = (float)v;
+}
+__global__ void k_reduce_full(int op, const float* in, int64_t n, double* part) {
+  double v = red_ident(op);
+  GRID_STRIDE(i, n) v = red_op(op, v, red_load(op, in[i]));
+  v = block_reduce(op, v);
+  if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+__global__ void k_reduce_final(int op, const double* part, int np, float* out) {
+  double v = red_ident(op);
+  for (int i = threadIdx.x; i < np; i += blockDim.x) v = red_op(op, v, part[i]);
+  v = block_reduce(op, v);
+  if (threadIdx.x == 0) out[0] = (float)v;
+}
+
+static double* g_red_part[64] = {nullptr};
+float gpu_reduce(int operation, float* input, float* dev2, float* host2, int blocks, int threads, int N) {
+  MMX_ABORT_ON(operation < 1 || operation > 5, "gpu_reduce: unknown operation %d", operation);
+  ABI_ASSERT(N > 0 && blocks > 0, "gpu_reduce");
+  (void)threads;
+  int dev = 0;
+  GK_CHECK(cudaGetDevice(&dev));
+  const int NP = 1024;
+  if (!g_red_part[dev & 63]) GK_CHECK(cudaMalloc(&g_red_part[dev & 63], sizeof(double) * NP));
+  int nb = ew_grid(N);
+  if (nb > NP) nb = NP;
+  k_reduce_full<<<nb, 256>>>(operation, input, N, g_red_part[dev & 63]);
+  GK_LAUNCHED();
+  k_reduce_final<<<1, 1024>>>(operation, g_red_part[dev & 63], nb, dev2);
+  GK_LAUNCHED();
+  GK_CHECK(cudaMemcpy(host2, dev2, sizeof(float), cudaMemcpyDeviceToHost));
+  GK_SYNC();
+  return host2[0];
+}
+
+static void partial(int op, float* in, float* out, int blocks, int threads, int N) {
+  ABI_ASSERT(blocks > 0 && threads > 0 && N > 0, "gpu_partial_*");
+  k_partial<<<blocks, 256>>>(op, in, out, N, 2LL * threads, blocks);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_partial_sums(float* in, float* out, int blocks, int threads, int N) { partial(REDUCE_ADD, in, out, blocks, threads, N); }
+void gpu_partial_sumabs(float* in, float* out, int blocks, int threads, int N) { partial(REDUCE_SUMABS, in, out, blocks, threads, N); }
+void gpu_partial_max(float* in, float* out, int blocks, int threads, int N) { partial(REDUCE_MAX, in, out, blocks, threads, N); }
+void gpu_partial_min(float* in, float* out, int blocks, int threads, int N) { partial(REDUCE_MIN, in, out, blocks, threads, N); }
+void gpu_partial_maxabs(float* in, float* out, int blocks, int threads, int N) { partial(REDUCE_MAXABS, in, out, blocks, threads, N); }
+int isPow2(unsigned int x) { return (x & (x - 1)) == 0; }
+
+// ---------------------------------------------------------------------
+// exchange stencils (gpu_exch1.cu): h += Laplacian(m), zero outside the
+// grid unless periodic, in the reference's summation order
+// ---------------------------------------------------------------------
+struct Exch {
+  int N0, N1, N2;
+  int p0, p1, p2;
+  float c0, c1, c2;    // 1/h^2 (6 ngbr) or 4/3/h^2 (12 ngbr)
+  float d0, d1, d2;    // -1/12/h^2 (12 ngbr)
+  float cc;            // centre
+  int twelve, is2d;
+};
+__device__ __forceinline__ float nb(const float* m, const Exch& e, int i, int j, int k) {
+  if (i < 0 || i >= e.N0) { if (!e.p0) return 0.f; i = (i + 2 * e.N0) % e.N0; }
+  if (j < 0 || j >= e.N1) { if (!e.p1) return 0.f; j = (j + 2 * e.N1) % e.N1; }
+  if (k < 0 || k >= e.N2) { if (!e.p2) return 0.f; k = (k + 2 * e.N2) % e.N2; }
+  return m[((int64_t)i * e.N1 + j) * e.N2 + k];
+}
+__global__ void k_exch(const float* m, float* h, Exch e) {
+  int64_t n = (int64_t)e.N0 * e.N1 * e.N2;
+  GRID_STRIDE(g, n) {
+    int k = (int)(g % e.N2);
+    int j = (int)((g / e.N2) % e.N1);
+    int i = (int)(g / ((int64_t)e.N1 * e.N2));
+    float r = FM(e.cc, m[g]);
+    if (!e.twelve) {
+      if (!e.is2d) {
+        r = FA(r, FM(e.c0, nb(m, e, i - 1, j, k)));
+        r = FA(r, FM(e.c0, nb(m, e, i + 1, j, k)));
+      }
+      r = FA(r, FM(e.c1, nb(m, e, i, j - 1, k)));
+      r = FA(r, FM(e.c1, nb(m, e, i, j + 1, k)));
+      r = FA(r, FM(e.c2, nb(m, e, i, j, k - 1)));
+      r = FA(r, FM(e.c2, nb(m, e, i, j, k + 1)));
+    } else if (e.is2d) {  // gpu_exch1.cu:377-386
+      r = FA(r, FM(e.c1, nb(m, e, i, j - 1, k)));
+      r = FA(r, FM(e.d1, nb(m, e, i, j - 2, k)));
+      r = FA(r, FM(e.c1, nb(m, e, i, j + 1, k)));
+      r = FA(r, FM(e.d1, nb(m, e, i, j + 2, k)));
+      r = FA(r, FM(e.c2, nb(m, e, i, j, k - 1)));
+      r = FA(r, FM(e.d2, nb(m, e, i, j, k - 2)));
+      r = FA(r, FM(e.c2, nb(m, e, i, j, k + 1)));
+      r = FA(r, FM(e.d2, nb(m, e, i, j, k + 2)));
+    } else {  // gpu_exch1.cu:556-569
+      r = FA(r, FM(e.d0, nb(m, e, i - 2, j, k)));
+      r = FA(r, FM(e.c0, nb(m, e, i - 1, j, k)));
+      r = FA(r, FM(e.c0, nb(m, e, i + 1, j, k)));
+      r = FA(r, FM(e.d0, nb(m, e, i + 2, j, k)));
+      r = FA(r, FM(e.d1, nb(m, e, i, j - 2, k)));
+      r = FA(r, FM(e.c1, nb(m, e, i, j - 1, k)));
+      r = FA(r, FM(e.c1, nb(m, e, i, j + 1, k)));
+      r = FA(r, FM(e.d1, nb(m, e, i, j + 2, k)));
+      r = FA(r, FM(e.d2, nb(m, e, i, j, k - 2)));
+      r = FA(r, FM(e.c2, nb(m, e, i, j, k - 1)));
+      r = FA(r, FM(e.c2, nb(m, e, i, j, k + 1)));
+      r = FA(r, FM(e.d2, nb(m, e, i, j, k + 2)));
+    }
+    h[g] = FA(h[g], r);
+  }
+}
+static inline float hdiv(float a, float b) { volatile float r = a / b; return r; }
+static inline float hsub(float a, float b) { volatile float r = a - b; return r; }
+static void exch_launch(float* m, float* h, int* size, int* periodic, float* cs, int twelve, int is2d) {
+  Exch e;
+  memset(&e, 0, sizeof(e));
+  e.N0 = is2d ? 1 : size[0];
+  e.N1 = size[1];
+  e.N2 = size[2];
+  e.p0 = periodic[0];
+  e.p1 = periodic[1];
+  e.p2 = periodic[2];
+  e.twelve = twelve;
+  e.is2d = is2d;
+  if (!twelve) {
+    e.c0 = hdiv(hdiv(1.f, cs[0]), cs[0]);
+    e.c1 = hdiv(hdiv(1.f, cs[1]), cs[1]);
+    e.c2 = hdiv(hdiv(1.f, cs[2]), cs[2]);
+    float t1 = hdiv(hdiv(-2.f, cs[1]), cs[1]), t2 = hdiv(hdiv(2.f, cs[2]), cs[2]);
+    if (is2d) e.cc = hsub(t1, t2);
+    else e.cc = hsub(hsub(hdiv(hdiv(-2.f, cs[0]), cs[0]), hdiv(hdiv(2.f, cs[1]), cs[1])), t2);
+  } else {
+    const float a = hdiv(4.0f, 3.0f), b = hdiv(-1.0f, 12.0f), c = hdiv(5.0f, 2.0f);
+    e.c0 = hdiv(hdiv(a, cs[0]), cs[0]);
+    e.c1 = hdiv(hdiv(a, cs[1]), cs[1]);
+    e.c2 = hdiv(hdiv(a, cs[2]), cs[2]);
+    e.d0 = hdiv(hdiv(b, cs[0]), cs[0]);
+    e.d1 = hdiv(hdiv(b, cs[1]), cs[1]);
+    e.d2 = hdiv(hdiv(b, cs[2]), cs[2]);
+    float t2 = hdiv(hdiv(c, cs[2]), cs[2]);
+    if (is2d) e.cc = hsub(hdiv(hdiv(-c, cs[1]), cs[1]), t2);
+    else e.cc = hsub(hsub(hdiv(hdiv(-c, cs[0]), cs[0]), hdiv(hdiv(c, cs[1]), cs[1])), t2);
+  }
+  int64_t n = (int64_t)e.N0 * e.N1 * e.N2;
+  k_exch<<<ew_grid(n), EW_BLOCK>>>(m, h, e);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+void gpu_add_6NGBR_exchange_3D_geometry(float* m, float* h, int* size, int* periodic, float* cellSize) {
+  exch_launch(m, h, size, periodic, cellSize, 0, 0);
+}
+void gpu_add_6NGBR_exchange_2D_geometry(float* m, float* h, int* size, int* periodic, float* cellSize) {
+  exch_launch(m, h, size, periodic, cellSize, 0, 1);
+}
+void gpu_add_12NGBR_exchange_3D_geometry(float* m, float* h, int* size, int* periodic, float* cellSize) {
+  exch_launch(m, h, size, periodic, cellSize, 1, 0);
+}
+void gpu_add_12NGBR_exchange_2D_geometry(float* m, float* h, int* size, int* periodic, float* cellSize) {
+  exch_launch(m, h, size, periodic, cellSize, 1, 1);
+}
+// gpu_exch1.cu:21-57
+void gpu_add_exch(float* m, float* h, int* size, int* periodic, int* exchInConv, float* cellSize, int type) {
+  if (exchInConv[0] != 0 && exchInConv[1] != 0 && exchInConv[2] != 0) return;
+  int N = size[0] * size[1] * size[2];
+  for (int i = 0; i < 3; i++) {
+    if (exchInConv[i] != 0) continue;
+    float* mc = m + (int64_t)i * N;
+    float* hc = h + (int64_t)i * N;
+    if (type == 6) {
+      if (size[0] == 1) gpu_add_6NGBR_exchange_2D_geometry(mc, hc, size, periodic, cellSize);
+      else gpu_add_6NGBR_exchange_3D_geometry(mc, hc, size, periodic, cellSize);
+    } else if (type == 12) {
+      if (size[0] == 1) gpu_add_12NGBR_exchange_2D_geometry(mc, hc, size, periodic, cellSize);
+      else gpu_add_12NGBR_exchange_3D_geometry(mc, hc, size, periodic, cellSize);
+    } else {
+      MMX_ABORT_ON(1, "abort: no valid exchType %d", type);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------
+// linear anisotropy, semi-analytical step, spin-transfer torque
+// ---------------------------------------------------------------------
+__global__ void k_lin_anis(float* hx, float* hy, float* hz, const float* mx, const float* my, const float* mz,
+                           const float* kxx, const float* kyy, const float* kzz, const float* kyz, const float* kxz,
+                           const float* kxy, int64_t n) {
+  GRID_STRIDE(i, n) {
+    float Mx = mx[i], My = my[i], Mz = mz[i];
+    hx[i] = FA(hx[i], FA(FA(FM(Mx, kxx[i]), FM(My, kxy[i])), FM(Mz, kxz[i])));
+    hy[i] = FA(hy[i], FA(FA(FM(Mx, kxy[i]), FM(My, kyy[i])), FM(Mz, kyz[i])));
+    hz[i] = FA(hz[i], FA(FA(FM(Mx, kxz[i]), FM(My, kyz[i])), FM(Mz, kzz[i])));
+  }
+}
+void gpu_add_lin_anisotropy(float* hx, float* hy, float* hz, float* mx, float* my, float* mz, float* kxx, float* kyy,
+                            float* kzz, float* kyz, float* kxz, float* kxy, int N) {
+  k_lin_anis<<<ew_grid(N), EW_BLOCK>>>(hx, hy, hz, mx, my, mz, kxx, kyy, kzz, kyz, kxz, kxy, N);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+
+// exact precession-damping rotation about h (gpu_anal.cu:23-90)
+__global__ void k_anal(const float* mi, float* mo, const float* h, float dt, float alpha, int64_t n) {
+  GRID_STRIDE(i, n) {
+    float mx = mi[i], my = mi[n + i], mz = mi[2 * n + i];
+    if (mx == 0.f && my == 0.f && mz == 0.f) continue;
+    float hx = h[i], hy = h[n + i], hz = h[2 * n + i];
+    float r0, r1, r2, r3, r4, r5, r6, r8, hxyz_r;
+    if (hx == 0.f && hy == 0.f) {
+      r0 = 0.f; r1 = 0.f; r2 = -1.f; r3 = 0.f; r4 = 1.f; r5 = 0.f; r6 = 1.f; r8 = 0.f;
+      hxyz_r = 1.f / hz;
+    } else {
+      float t = hx * hx + hy * hy;
+      float hxy_r = 1.f / sqrtf(t);
+      hxyz_r = 1.f / sqrtf(t + hz * hz);
+      r0 = hx * hxyz_r;
+      r1 = -hy * hxy_r;
+      r2 = -r0 * hz * hxy_r;
+      r3 = hy * hxyz_r;
+      r4 = hx * hxy_r;
+      r5 = r1 * hz * hxyz_r;
+      r6 = hz * hxyz_r;
+      r8 = hxyz_r / hxy_r;
+    }
+    float mxr = mx * r0 + my * r3 + mz * r6;
+    float myr = mx * r1 + my * r4;
+    float mzr = mx * r2 + my * r5 + mz * r8;
+    float qt = dt / (1 + alpha * alpha);
+    float aqt = alpha * qt;
+    float ex = expf(aqt / hxyz_r);
+    float sn, cs;
+    sincosf(qt / hxyz_r, &sn, &cs);
+    float den = ex * (1.f + mxr) + (1.f - mxr) / ex;
+    float nx = (ex * (1.f + mxr) - (1.f - mxr) / ex) / den;
+    float ny = 2.f * (myr * cs - mzr * sn) / den;
+    float nz = 2.f * (myr * sn + mzr * cs) / den;
+    mo[i] = nx * r0 + ny * r1 + nz * r2;
+    mo[n + i] = nx * r3 + ny * r4 + nz * r5;
+    mo[2 * n + i] = nx * r6 + nz * r8;
+  }
+}
+void gpu_anal_fw_step(float dt, float alpha, int Ntot, float* m_in, float* m_out, float* h) {
+  k_anal<<<ew_grid(Ntot), EW_BLOCK>>>(m_in, m_out, h, dt, alpha, Ntot);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+__global__ void k_mean_h(float* h1, const float* h2, int64_t n) { GRID_STRIDE(i, n) h1[i] = FM(0.5f, FA(h1[i], h2[i])); }
+void gpu_anal_pc_mean_h(float* h1, float* h2, int Ntot) {
+  k_mean_h<<<ew_grid(Ntot), EW_BLOCK>>>(h1, h2, Ntot);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+
+// Zhang-Li spin-transfer torque (gpu_spintorque.cu:24-189), including the
+// reference's edge handling: at the upper X edge the centre replaces the
+// lower neighbour and the upper one stays zero (gpu_spintorque.cu:73-79).
+__global__ void k_stt(const float* m, float* h, float alpha, float beta, float eps, float ux0, float uy0, float uz0,
+                      const float* jmap, float dtg, int N0, int N1, int N2) {
+  int64_t n = (int64_t)N0 * N1 * N2;
+  GRID_STRIDE(I, n) {
+    int k = (int)(I % N2);
+    int j = (int)((I / N2) % N1);
+    int i = (int)(I / ((int64_t)N1 * N2));
+    float ux = ux0, uy = uy0, uz = uz0;
+    if (jmap) {
+      ux *= jmap[I];
+      uy *= jmap[n + I];
+      uz *= jmap[2 * n + I];
+    }
+    const float *mx = m, *my = m + n, *mz = m + 2 * n;
+    float x1 = 0.f, x2 = 0.f, y1 = 0.f, y2 = 0.f, z1 = 0.f, z2 = 0.f;
+    int64_t idx;
+    idx = i - 1 >= 0 ? I - (int64_t)N1 * N2 : I;
+    x1 = mx[idx]; y1 = my[idx]; z1 = mz[idx];
+    if (i + 1 < N0) { idx = I + (int64_t)N1 * N2; x2 = mx[idx]; y2 = my[idx]; z2 = mz[idx]; }
+    else { x1 = mx[I]; y1 = my[I]; z1 = mz[I]; }
+    float dx = ux * (x2 - x1), dy = ux * (y2 - y1), dz = ux * (z2 - z1);
+    idx = j - 1 >= 0 ? I - N2 : I;
+    x1 = mx[idx]; y1 = my[idx]; z1 = mz[idx];
+    idx = j + 1 < N1 ? I + N2 : I;
+    x2 = mx[idx]; y2 = my[idx]; z2 = mz[idx];
+    dx += uy * (x2 - x1); dy += uy * (y2 - y1); dz += uy * (z2 - z1);
+    idx = k - 1 >= 0 ? I - 1 : I;
+    x1 = mx[idx]; y1 = my[idx]; z1 = mz[idx];
+    idx = k + 1 < N2 ? I + 1 : I;
+    x2 = mx[idx]; y2 = my[idx]; z2 = mz[idx];
+    dx += uz * (x2 - x1); dy += uz * (y2 - y1); dz += uz * (z2 - z1);
+    float Hx = h[I], Hy = h[n + I], Hz = h[2 * n + I];
+    float Mx = mx[I], My = my[I], Mz = mz[I];
+    float Hpx = Hx + eps * dx, Hpy = Hy + eps * dy, Hpz = Hz + eps * dz;
+    float px = -My * Hpz + Hpy * Mz, py = Mx * Hpz - Hpx * Mz, pz = -Mx * Hpy + Hpx * My;
+    float Hdx = alpha * Hx + beta * dx, Hdy = alpha * Hy + beta * dy, Hdz = alpha * Hz + beta * dz;
+    float qx = -My * Hdz + Hdy * Mz, qy = Mx * Hdz - Hdx * Mz, qz = -Mx * Hdy + Hdx * My;
+    float rx = My * qz - qy * Mz, ry = -Mx * qz + qx * Mz, rz = Mx * qy - qx * My;
+    h[I] = dtg * (-px + rx);
+    h[n + I] = dtg * (-py + ry);
+    h[2 * n + I] = dtg * (-pz + rz);
+  }
+}
+void gpu_spintorque_deltaM(float* m, float* h, float alpha, float beta, float epsillon, float* u, float* jmap,
+                           float dt_gilb, int N0, int N1, int N2) {
+  int64_t n = (int64_t)N0 * N1 * N2;
+  k_stt<<<ew_grid(n), EW_BLOCK>>>(m, h, alpha, beta, epsillon, u[0], u[1], u[2], jmap, dt_gilb, N0, N1, N2);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+__global__ void k_dir_diff(float ux, float uy, float uz, const float* in, float* out, int N0, int N1, int N2) {
+  int64_t n = (int64_t)N0 * N1 * N2;
+  GRID_STRIDE(I, n) {
+    int k = (int)(I % N2);
+    int j = (int)((I / N2) % N1);
+    int i = (int)(I / ((int64_t)N1 * N2));
+    float m0 = in[I];
+    float a = i - 1 >= 0 ? in[I - (int64_t)N1 * N2] : m0, b = i + 1 < N0 ? in[I + (int64_t)N1 * N2] : m0;
+    float r = ux * (b - a);
+    a = j - 1 >= 0 ? in[I - N2] : m0;
+    b = j + 1 < N1 ? in[I + N2] : m0;
+    r += uy * (b - a);
+    a = k - 1 >= 0 ? in[I - 1] : m0;
+    b = k + 1 < N2 ? in[I + 1] : m0;
+    r += uz * (b - a);
+    out[I] = r;
+  }
+}
+void gpu_directionial_diff(float ux, float uy, float uz, float* in, float* out, int N0, int N1, int N2) {
+  int64_t n = (int64_t)N0 * N1 * N2;
+  k_dir_diff<<<ew_grid(n), EW_BLOCK>>>(ux, uy, uz, in, out, N0, N1, N2);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+
+// ---------------------------------------------------------------------
+// Gaussian noise: Philox-4x32-10 counter-based generator (Salmon et al.,
+// SC'11) and the Box-Muller transform; the counter advances per call so
+// successive calls give fresh numbers.
+// ---------------------------------------------------------------------
+__device__ __forceinline__ uint4 philox_round(uint4 c, uint2 k) {
+  unsigned int hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+  unsigned int hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+  return make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+}
+__device__ uint4 philox10(uint4 c, uint2 k) {
+  for (int r = 0; r < 10; r++) {
+    c = philox_round(c, k);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+__global__ void k_gauss(float* out, float mean, float sd, int64_t n, unsigned long long seed, unsigned long long ctr) {
+  int64_t pairs = (n + 1) / 2;
+  GRID_STRIDE(p, pairs) {
+    uint4 c = make_uint4((unsigned)p, (unsigned)(p >> 32), (unsigned)ctr, (unsigned)(ctr >> 32));
+    uint4 r = philox10(c, make_uint2((unsigned)seed, (unsigned)(seed >> 32)));
+    float u1 = ((float)(r.x >> 8) + 1.f) * (1.f / 16777216.f);  // (0, 1]
+    float u2 = (float)(r.y >> 8) * (1.f / 16777216.f);
+    float rad = sqrtf(-2.f * logf(u1));
+    float s, c2;
+    sincospif(2.f * u2, &s, &c2);
+    out[2 * p] = mean + sd * rad * c2;
+    if (2 * p + 1 < n) out[2 * p + 1] = mean + sd * rad * s;
+  }
+}
+static unsigned long long g_noise_ctr = 0;
+void gpu_gaussian_noise(float* devData, float mean, float stddev, int n) {
+  ABI_ASSERT(n > 0, "gpu_gaussian_noise");
+  k_gauss<<<ew_grid((n + 1) / 2), EW_BLOCK>>>(devData, mean, stddev, n, 0ULL, g_noise_ctr++);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+
+// ---------------------------------------------------------------------
+// complex transposes (gpu_transpose.cu:34-125)
+// ---------------------------------------------------------------------
+// YZ: per plane x, (N1 rows of N2c) -> (N2c rows of N1) with N2c = N2/2
+__global__ void k_tr_yz(const float2* in, float2* out, int A, int B, int planes) {
+  int64_t n = (int64_t)planes * A * B;
+  GRID_STRIDE(e, n) {
+    int j = (int)(e % A);  // output column index
+    int i = (int)((e / A) % B);
+    int x = (int)(e / ((int64_t)A * B));
+    out[(int64_t)x * A * B + (int64_t)i * A + j] = in[(int64_t)x * A * B + (int64_t)j * B + i];
+  }
+}
+void gpu_transpose_complex_YZ(float* input, float* output, int N1, int N2, int N0) {
+  // the reference's kernel reads input[x*N1*N2 + J*N1 + I] with N1 := N2/2
+  // complex columns and N2 := N1 rows (gpu_transpose.cu:74-79)
+  int cols = N2 / 2, rows = N1;
+  int64_t n = (int64_t)N0 * cols * rows;
+  k_tr_yz<<<ew_grid(n), EW_BLOCK>>>((const float2*)input, (float2*)output, rows, cols, N0);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+// XZ: output[k][y][x] = input[x][y][k] over (N0 x N1 x N2/2 complex)
+__global__ void k_tr_xz(const float2* in, float2* out, int N0, int N1, int N2c) {
+  int64_t n = (int64_t)N0 * N1 * N2c;
+  GRID_STRIDE(e, n) {
+    int k = (int)(e % N2c);
+    int y = (int)((e / N2c) % N1);
+    int x = (int)(e / ((int64_t)N1 * N2c));
+    out[((int64_t)k * N1 + y) * N0 + x] = in[e];
+  }
+}
+void gpu_transpose_complex_XZ(float* input, float* output, int N0, int N1, int N2) {
+  int N2c = N2 / 2;
+  int64_t n = (int64_t)N0 * N1 * N2c;
+  k_tr_xz<<<ew_grid(n), EW_BLOCK>>>((const float2*)input, (float2*)output, N0, N1, N2c);
+  GK_LAUNCHED();
+  GK_SYNC();
+}
+

@@ -1,0 +1,1169 @@
+// Fused LLG solver (extended mmx_* ABI).
+//
+// One effective-field evaluation of an (N0,N1,N2) grid padded to
+// (P0,P1,P2) runs as
+//   3D: Zf -> Yf -> Xconv -> Yi -> Zi+epilogue        (5 kernels)
+//   2D: Zf -> Yconv -> Zi+epilogue                     (3 kernels)
+// over one spectrum buffer S[3][N0][P1][HZ] (complex, HZ = P2/2 + 1):
+//  * Zf  : R2C of the magnetisation rows, all three components (zero
+//          padding in Z implicit, only the N0 x N1 data rows exist);
+//  * Yf  : column FFT of the N1 data rows of each (component, x) plane;
+//  * Xconv: for each (ky, kz) column, forward X FFT of the N0 data planes,
+//          multiplication by the symmetric demag(+exchange) kernel and
+//          inverse X FFT, writing only the N0 planes the next pass reads
+//          (in 2D the Y transform plays this role);
+//  * Yi  : inverse column FFT, only the N1 output rows are stored;
+//  * Zi+epilogue: C2R of the three components of a row in shared memory,
+//          then the local fields, the LLG torque and the solver stage
+//          update per cell (Heun predictor/corrector, RK stage, or just
+//          the field).
+// The kernel spectrum is real; it is stored as one octant (kx <= P0/2,
+// ky <= P1/2, all kz) and unfolded with the parity of each component
+// (diagonal components even, XY odd in kx,ky, XZ odd in kx, YZ odd in ky).
+#include <math.h>
+#include <string.h>
+#include <string>
+#include <vector>
+
+#include "demag_gpu.cuh"
+#include "fft_passes.cuh"
+#include "llg_ops.cuh"
+#include "../../include/mmx.h"
+
+static thread_local std::string g_err = "";
+void mmx_set_error(const char* msg) { g_err = msg ? msg : ""; }
+extern "C" const char* mmx_last_error(void) { return g_err.c_str(); }
+
+int mmx_sm_count() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+// ---------------------------------------------------------------------
+// Kernel octant
+// ---------------------------------------------------------------------
+struct KernOct {
+  const float* kh;  // [6][O0][O1][HZ]
+  int O0, O1, HZ, P0, P1;
+  int64_t cs;       // component stride
+};
+
+__global__ void k_extract_octant(const float2* __restrict__ spec, float* __restrict__ kh, int O0, int O1, int P1,
+                                 int HZ, float norm) {
+  int64_t n = (int64_t)O0 * O1 * HZ;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    int kz = (int)(e % HZ);
+    int ky = (int)((e / HZ) % O1);
+    int kx = (int)(e / ((int64_t)HZ * O1));
+    kh[e] = __fmul_rn(spec[((int64_t)kx * P1 + ky) * HZ + kz].x, norm);
+  }
+}
+
+__device__ __forceinline__ void kern_at(const KernOct& K, int kx, int ky, int kz, float& Kxx, float& Kyy,
+                                        float& Kzz, float& Kyz, float& Kxz, float& Kxy) {
+  int fx = kx <= K.P0 / 2 ? kx : K.P0 - kx;
+  int fy = ky <= K.P1 / 2 ? ky : K.P1 - ky;
+  bool nx = kx > K.P0 / 2, ny = ky > K.P1 / 2;
+  int64_t o = ((int64_t)fx * K.O1 + fy) * K.HZ + kz;
+  Kxx = __ldg(K.kh + o);
+  Kyy = __ldg(K.kh + K.cs + o);
+  Kzz = __ldg(K.kh + 2 * K.cs + o);
+  Kyz = __ldg(K.kh + 3 * K.cs + o);
+  Kxz = __ldg(K.kh + 4 * K.cs + o);
+  Kxy = __ldg(K.kh + 5 * K.cs + o);
+  if (ny) Kyz = -Kyz;
+  if (nx) Kxz = -Kxz;
+  if (nx != ny) Kxy = -Kxy;
+}
+
+// H = K M per bin in the order of gpu_kernelmul6 (gpu_kernmul.cu:51-58)
+__device__ __forceinline__ void kmul6(float2& mx, float2& my, float2& mz, float Kxx, float Kyy, float Kzz, float Kyz,
+                                      float Kxz, float Kxy) {
+  float2 hx, hy, hz;
+  hx.x = FA(FA(FM(mx.x, Kxx), FM(my.x, Kxy)), FM(mz.x, Kxz));
+  hx.y = FA(FA(FM(mx.y, Kxx), FM(my.y, Kxy)), FM(mz.y, Kxz));
+  hy.x = FA(FA(FM(mx.x, Kxy), FM(my.x, Kyy)), FM(mz.x, Kyz));
+  hy.y = FA(FA(FM(mx.y, Kxy), FM(my.y, Kyy)), FM(mz.y, Kyz));
+  hz.x = FA(FA(FM(mx.x, Kxz), FM(my.x, Kyz)), FM(mz.x, Kzz));
+  hz.y = FA(FA(FM(mx.y, Kxz), FM(my.y, Kyz)), FM(mz.y, Kzz));
+  mx = hx;
+  my = hy;
+  mz = hz;
+}
+// 2D: Kxy = Kxz = 0 (gpu_kernmul.cu:114-119)
+__device__ __forceinline__ void kmul4(float2& mx, float2& my, float2& mz, float Kxx, float Kyy, float Kzz,
+                                      float Kyz) {
+  float2 hx, hy, hz;
+  hx.x = FM(mx.x, Kxx);
+  hx.y = FM(mx.y, Kxx);
+  hy.x = FA(FM(my.x, Kyy), FM(mz.x, Kyz));
+  hy.y = FA(FM(my.y, Kyy), FM(mz.y, Kyz));
+  hz.x = FA(FM(my.x, Kyz), FM(mz.x, Kzz));
+  hz.y = FA(FM(my.y, Kyz), FM(mz.y, Kzz));
+  mx = hx;
+  my = hy;
+  mz = hz;
+}
+
+// ---------------------------------------------------------------------
+// Xconv (3D): columns (ky, kz) flattened, tile of tk columns x 3 comps.
+// Tile layout: element x of line (c, t) at sm[x * 3tk + c * tk + t].
+// ---------------------------------------------------------------------
+template <int THREADS, int EPT, bool POW2>
+__global__ void FFT_BOUNDS(THREADS) k_xconv(float2* __restrict__ S, LineFFT fx, KernOct K, int N0, int P1, int HZ,
+                                               int64_t CS, int tk) {
+  extern __shared__ float2 sm[];
+  const int P0 = fx.L;
+  const int ncol = P1 * HZ;
+  const int col0 = blockIdx.x * tk;
+  const int nc = min(tk, ncol - col0);
+  const int nl = 3 * tk;
+  const int64_t plane = (int64_t)P1 * HZ;
+  for (int e = threadIdx.x; e < P0 * nl; e += THREADS) {
+    int i = e / nl, l = e - i * nl;
+    int c = l / tk, t = l - c * tk;
+    float2 v = make_float2(0.f, 0.f);
+    if (i < N0 && t < nc) v = S[c * CS + i * plane + col0 + t];
+    sm[e] = v;
+  }
+  __syncthreads();
+  tile_fft<EPT, POW2>(sm, fx, nl, nl, 1, true, false);
+  for (int e = threadIdx.x; e < P0 * tk; e += THREADS) {
+    int kx = e / tk, t = e - kx * tk;
+    if (t >= nc) continue;
+    int col = col0 + t;
+    int ky = col / HZ, kz = col - ky * HZ;
+    float Kxx, Kyy, Kzz, Kyz, Kxz, Kxy;
+    kern_at(K, kx, ky, kz, Kxx, Kyy, Kzz, Kyz, Kxz, Kxy);
+    float2* b = sm + kx * nl + t;
+    float2 mx = b[0], my = b[tk], mz = b[2 * tk];
+    kmul6(mx, my, mz, Kxx, Kyy, Kzz, Kyz, Kxz, Kxy);
+    b[0] = mx;
+    b[tk] = my;
+    b[2 * tk] = mz;
+  }
+  __syncthreads();
+  tile_fft<EPT, POW2>(sm, fx, nl, nl, 1, true, true);
+  for (int e = threadIdx.x; e < N0 * nl; e += THREADS) {
+    int i = e / nl, l = e - i * nl;
+    int c = l / tk, t = l - c * tk;
+    if (t < nc) S[c * CS + i * plane + col0 + t] = sm[e];
+  }
+}
+
+// Yconv (2D, N0 = P0 = 1): columns kz, tile of tk columns x 3 comps.
+template <int THREADS, int EPT, bool POW2>
+__global__ void FFT_BOUNDS(THREADS) k_yconv2d(float2* __restrict__ S, LineFFT fy, KernOct K, int N1, int HZ,
+                                                 int64_t CS, int tk) {
+  extern __shared__ float2 sm[];
+  const int P1 = fy.L;
+  const int kz0 = blockIdx.x * tk;
+  const int nc = min(tk, HZ - kz0);
+  const int nl = 3 * tk;
+  for (int e = threadIdx.x; e < P1 * nl; e += THREADS) {
+    int i = e / nl, l = e - i * nl;
+    int c = l / tk, t = l - c * tk;
+    float2 v = make_float2(0.f, 0.f);
+    if (i < N1 && t < nc) v = S[c * CS + (int64_t)i * HZ + kz0 + t];
+    sm[e] = v;
+  }
+  __syncthreads();
+  tile_fft<EPT, POW2>(sm, fy, nl, nl, 1, true, false);
+  for (int e = threadIdx.x; e < P1 * tk; e += THREADS) {
+    int ky = e / tk, t = e - ky * tk;
+    if (t >= nc) continue;
+    float Kxx, Kyy, Kzz, Kyz, Kxz, Kxy;
+    kern_at(K, 0, ky, kz0 + t, Kxx, Kyy, Kzz, Kyz, Kxz, Kxy);
+    float2* b = sm + ky * nl + t;
+    float2 mx = b[0], my = b[tk], mz = b[2 * tk];
+    kmul4(mx, my, mz, Kxx, Kyy, Kzz, Kyz);
+    b[0] = mx;
+    b[tk] = my;
+    b[2 * tk] = mz;
+  }
+  __syncthreads();
+  tile_fft<EPT, POW2>(sm, fy, nl, nl, 1, true, true);
+  for (int e = threadIdx.x; e < N1 * nl; e += THREADS) {
+    int i = e / nl, l = e - i * nl;
+    int c = l / tk, t = l - c * tk;
+    if (t < nc) S[c * CS + (int64_t)i * HZ + kz0 + t] = sm[e];
+  }
+}
+
+// ---------------------------------------------------------------------
+// Zi + epilogue: inverse Z (C2R) of the three components of R rows in
+// shared memory, then the per-cell solver update.
+// ---------------------------------------------------------------------
+enum { EPI_FIELD = 0, EPI_HEUN1 = 1, EPI_HEUN2 = 2, EPI_TORQUE = 3, EPI_RK = 4 };
+
+#define RK_MAXS 7
+struct RKCoef {
+  float a[RK_MAXS];   // row a[i+1][0..i] (next stage input), or b for the final stage
+  float b2[RK_MAXS];  // lower-order weights (final stage, adaptive)
+  int nk;             // number of k's combined
+  int final_stage;    // 1: produce m_high / m_low / error
+  int adaptive;
+};
+
+struct EpiArgs {
+  int N1, N2;
+  int64_t n;            // cells per component
+  LocalField lf;
+  float alpha, dtg;
+  const float* m_in;    // magnetisation at which the field was evaluated
+  float* out0;
+  float* out1;
+  const float* aux0;
+  const float* aux1;
+  float* err;           // device scalar (maxabs target), may be null
+  const float* dt_dev;  // RK: device dt
+  float* kbuf[RK_MAXS]; // RK: stage torques
+  int stage;            // RK: index of this stage's k
+  RKCoef rk;
+};
+
+template <int THREADS, int EPT, bool POW2, int MODE>
+__global__ void FFT_BOUNDS(THREADS) k_zinv_epi(const float2* __restrict__ S, LineFFT fz,
+                                                  const float2* __restrict__ twP, int N0, int P1, int HZ, int64_t CS,
+                                                  int rows, int nrows_total, EpiArgs ea) {
+  extern __shared__ float2 sm[];
+  const int M = fz.L;
+  const int ld = M + 1;
+  const int nl = 3 * rows;
+  const int nt = THREADS;
+  const int r0 = blockIdx.x * rows;
+  const int nr = min(rows, nrows_total - r0);
+  const int N1 = ea.N1, N2 = ea.N2;
+  for (int e = threadIdx.x; e < nl * ld; e += nt) {
+    int l = e / ld, k = e - l * ld;
+    int r = l / 3, c = l - 3 * r;
+    float2 v = make_float2(0.f, 0.f);
+    if (r < nr) {
+      int gr = r0 + r;
+      int x = gr / N1, y = gr - x * N1;
+      v = S[c * CS + ((int64_t)x * P1 + y) * HZ + k];
+      if (k == 0 || k == M) v.y = 0.f;
+    }
+    sm[e] = v;
+  }
+  __syncthreads();
+  {
+    float2 v[EPT];
+#pragma unroll
+    for (int it = 0; it < EPT; it++) {
+      int e = it * nt + threadIdx.x;
+      if (e < nl * M) {
+        int l = e / M, k = e - l * M;
+        float2 Xk = sm[l * ld + k], Xm = sm[l * ld + (M - k)];
+        float2 A = make_float2(Xk.x + Xm.x, Xk.y - Xm.y);
+        float2 B = make_float2(Xk.x - Xm.x, Xk.y + Xm.y);
+        float2 w = __ldg(&twP[k]);
+        w.y = -w.y;
+        float2 C = cmul(B, w);
+        v[it] = make_float2(A.x - C.y, A.y + C.x);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < EPT; it++) {
+      int e = it * nt + threadIdx.x;
+      if (e < nl * M) {
+        int l = e / M, k = e - l * M;
+        sm[l * ld + k] = v[it];
+      }
+    }
+    __syncthreads();
+  }
+  tile_fft<EPT, POW2>(sm, fz, nl, 1, ld, false, true);
+
+  float lmax = 0.f;
+  for (int e = threadIdx.x; e < nr * N2; e += nt) {
+    int r = e / N2, z = e - r * N2;
+    int64_t g = (int64_t)(r0 + r) * N2 + z;
+    const float2* base = sm + (r * 3) * ld + (z >> 1);
+    float hx = (z & 1) ? base[0].y : base[0].x;
+    float hy = (z & 1) ? base[ld].y : base[ld].x;
+    float hz = (z & 1) ? base[2 * ld].y : base[2 * ld].x;
+    const int64_t n = ea.n;
+    float mx = ea.m_in[g], my = ea.m_in[n + g], mz = ea.m_in[2 * n + g];
+    llg_local(ea.lf, mx, my, mz, hx, hy, hz);
+    if (MODE == EPI_FIELD) {
+      ea.out0[g] = hx;
+      ea.out0[n + g] = hy;
+      ea.out0[2 * n + g] = hz;
+      continue;
+    }
+    llg_delta_m(mx, my, mz, hx, hy, hz, ea.alpha, ea.dtg);
+    if (MODE == EPI_TORQUE) {
+      ea.out0[g] = hx;
+      ea.out0[n + g] = hy;
+      ea.out0[2 * n + g] = hz;
+      if (ea.err) lmax = fmaxf(lmax, fmaxf(fabsf(hx), fmaxf(fabsf(hy), fabsf(hz))));
+    } else if (MODE == EPI_HEUN1) {
+      // t0 = torque*dt; m1est = normalize(m + t0)   (adaptive_heun.go:141-146)
+      ea.out0[g] = hx;
+      ea.out0[n + g] = hy;
+      ea.out0[2 * n + g] = hz;
+      float ex = FA(mx, hx), ey = FA(my, hy), ez = FA(mz, hz);
+      llg_normalize(ex, ey, ez);
+      ea.out1[g] = ex;
+      ea.out1[n + g] = ey;
+      ea.out1[2 * n + g] = ez;
+    } else if (MODE == EPI_HEUN2) {
+      // t = 0.5 t1 + 0.5 t0; m = normalize(m + t)   (adaptive_heun.go:148-154)
+      float tx = FA(FM(0.5f, hx), FM(0.5f, ea.aux0[g]));
+      float ty = FA(FM(0.5f, hy), FM(0.5f, ea.aux0[n + g]));
+      float tz = FA(FM(0.5f, hz), FM(0.5f, ea.aux0[2 * n + g]));
+      float nx = FA(ea.aux1[g], tx), ny = FA(ea.aux1[n + g], ty), nz = FA(ea.aux1[2 * n + g], tz);
+      llg_normalize(nx, ny, nz);
+      ea.out0[g] = nx;
+      ea.out0[n + g] = ny;
+      ea.out0[2 * n + g] = nz;
+      if (ea.err) {
+        // error = maxabs(m1est - m)   (adaptive_heun.go:158-160)
+        float d0 = fabsf(FA(mx, FM(-1.f, nx)));
+        float d1 = fabsf(FA(my, FM(-1.f, ny)));
+        float d2 = fabsf(FA(mz, FM(-1.f, nz)));
+        lmax = fmaxf(lmax, fmaxf(d0, fmaxf(d1, d2)));
+      }
+    } else if (MODE == EPI_RK) {
+      float kx = hx, ky = hy, kz = hz;
+      float* kd = ea.out0;
+      kd[g] = kx;
+      kd[n + g] = ky;
+      kd[2 * n + g] = kz;
+      const float dt = *ea.dt_dev;
+      const float* m0 = ea.aux0;  // step start magnetisation
+      float q[3] = {m0[g], m0[n + g], m0[2 * n + g]};
+      // next stage input (or m_high): m0 + sum_j (dt a_j) k_j, j in order
+#pragma unroll
+      for (int j = 0; j < RK_MAXS; j++) {
+        if (j >= ea.rk.nk) break;
+        float a = ea.rk.a[j];
+        if (a == 0.f) continue;
+        float c = FM(dt, a);
+        float k0, k1, k2;
+        if (j == ea.stage) { k0 = kx; k1 = ky; k2 = kz; }
+        else { k0 = ea.kbuf[j][g]; k1 = ea.kbuf[j][n + g]; k2 = ea.kbuf[j][2 * n + g]; }
+        q[0] = FA(q[0], FM(c, k0));
+        q[1] = FA(q[1], FM(c, k1));
+        q[2] = FA(q[2], FM(c, k2));
+      }
+      if (ea.rk.final_stage && ea.rk.adaptive) {
+        float lo[3] = {m0[g], m0[n + g], m0[2 * n + g]};
+#pragma unroll
+        for (int j = 0; j < RK_MAXS; j++) {
+          if (j >= ea.rk.nk) break;
+          float b = ea.rk.b2[j];
+          if (b == 0.f) continue;
+          float c = FM(b, dt);
+          float k0, k1, k2;
+          if (j == ea.stage) { k0 = kx; k1 = ky; k2 = kz; }
+          else { k0 = ea.kbuf[j][g]; k1 = ea.kbuf[j][n + g]; k2 = ea.kbuf[j][2 * n + g]; }
+          lo[0] = FA(lo[0], FM(c, k0));
+          lo[1] = FA(lo[1], FM(c, k1));
+          lo[2] = FA(lo[2], FM(c, k2));
+        }
+        float d0 = fabsf(FA(lo[0], FM(-1.f, q[0])));
+        float d1 = fabsf(FA(lo[1], FM(-1.f, q[1])));
+        float d2 = fabsf(FA(lo[2], FM(-1.f, q[2])));
+        lmax = fmaxf(lmax, fmaxf(d0, fmaxf(d1, d2)));
+      }
+      ea.out1[g] = q[0];
+      ea.out1[n + g] = q[1];
+      ea.out1[2 * n + g] = q[2];
+    }
+  }
+  if ((MODE == EPI_HEUN2 || MODE == EPI_RK || MODE == EPI_TORQUE) && ea.err) {
+    for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(ea.err, lmax);
+  }
+}
+
+// ---------------------------------------------------------------------
+// Small helper kernels
+// ---------------------------------------------------------------------
+__global__ void k_normalize3(float* __restrict__ m, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float x = m[i], y = m[n + i], z = m[2 * n + i];
+    llg_normalize(x, y, z);
+    m[i] = x;
+    m[n + i] = y;
+    m[2 * n + i] = z;
+  }
+}
+
+// maxabs of a 3n vector into *out (out must be zeroed first)
+__global__ void k_maxabs(const float* __restrict__ a, int64_t n, float* out) {
+  float v = 0.f;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v = fmaxf(v, fabsf(a[i]));
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, v);
+}
+
+// ---------------------------------------------------------------------
+// Solver object
+// ---------------------------------------------------------------------
+struct PassTimer {
+  std::string name;
+  double ms = 0;
+  long long launches = 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+};
+
+struct mmx_solver {
+  mmx_params p;
+  int N[3], P[3], HZ;
+  int64_t n;
+  int is2d;
+  BoxPlan bp;
+  float2* S = nullptr;
+  int64_t CS = 0;
+  float* kh = nullptr;
+  KernOct K;
+  float* m = nullptr;
+  float* t0 = nullptr;
+  float* m1 = nullptr;
+  float* scratch = nullptr;  // device scalars: [0] err, [1] torque, [2] dt
+  float* kb[RK_MAXS] = {nullptr};
+  float* mnew = nullptr;
+  // solver scalars (host mirror)
+  double time = 0;
+  float dt = 0;
+  float torque = 0, step_error = 0;
+  long long steps = 0;
+  int fsal_init = 0;
+  // tableau
+  int stages = 0, fsal = 0, adaptive = 0;
+  double errorder = 1;
+  float a[RK_MAXS][RK_MAXS], b[RK_MAXS], b2[RK_MAXS], c[RK_MAXS];
+  // graph
+  int use_graph = 0;
+  cudaGraphExec_t gexec = nullptr;
+  cudaStream_t gstream = nullptr;
+  // profiling
+  int profile = 0;
+  std::vector<PassTimer> timers;
+};
+
+static void set_tableau(mmx_solver* s) {
+  memset(s->a, 0, sizeof(s->a));
+  memset(s->b, 0, sizeof(s->b));
+  memset(s->b2, 0, sizeof(s->b2));
+  memset(s->c, 0, sizeof(s->c));
+  s->fsal = 0;
+  s->adaptive = 0;
+  switch (s->p.solver) {
+    case MMX_SOLVER_RK2:
+    case MMX_SOLVER_RK12:
+      s->stages = 2;
+      s->c[1] = 1.f; s->a[1][0] = 1.f; s->b[0] = .5f; s->b[1] = .5f;
+      if (s->p.solver == MMX_SOLVER_RK12) { s->adaptive = 1; s->errorder = 1.; s->b2[0] = 1.f; }
+      break;
+    case MMX_SOLVER_RK23:
+      s->stages = 4; s->fsal = 1;
+      s->c[1] = (float)(1. / 2.); s->c[2] = (float)(3. / 4.); s->c[3] = 1.f;
+      s->a[1][0] = (float)(1. / 2.);
+      s->a[2][1] = (float)(3. / 4.);
+      s->a[3][0] = (float)(2. / 9.); s->a[3][1] = (float)(1. / 3.); s->a[3][2] = (float)(4. / 9.);
+      s->b[0] = (float)(2. / 9.); s->b[1] = (float)(1. / 3.); s->b[2] = (float)(4. / 9.);
+      s->adaptive = 1; s->errorder = 2.;
+      s->b2[0] = (float)(7. / 24); s->b2[1] = (float)(1. / 4.); s->b2[2] = (float)(1. / 3.); s->b2[3] = (float)(1. / 8.);
+      break;
+    case MMX_SOLVER_RK4:
+      s->stages = 4;
+      s->c[1] = .5f; s->c[2] = .5f; s->c[3] = 1.f;
+      s->a[1][0] = .5f; s->a[2][1] = .5f; s->a[3][2] = 1.f;
+      s->b[0] = (float)(1. / 6.); s->b[1] = (float)(1. / 3.); s->b[2] = (float)(1. / 3.); s->b[3] = (float)(1. / 6.);
+      break;
+    case MMX_SOLVER_RKCK: {
+      s->stages = 6;
+      double c[6] = {0., 1. / 5., 3. / 10., 3. / 5., 1., 7. / 8.};
+      double a[6][6] = {{0}, {1. / 5.}, {3. / 40., 9. / 40.}, {3. / 10., -9. / 10., 6. / 5.},
+                        {-11. / 54., 5. / 2., -70. / 27., 35. / 27.},
+                        {1631. / 55296., 175. / 512., 575. / 13824., 44275. / 110592., 253. / 4096.}};
+      double b[6] = {37. / 378., 0, 250. / 621., 125. / 594., 0, 512. / 1771.};
+      double b2[6] = {2825. / 27648., 0, 18575. / 48384., 13525. / 55296., 277. / 14336., 1. / 4.};
+      for (int i = 0; i < 6; i++) {
+        s->c[i] = (float)c[i]; s->b[i] = (float)b[i]; s->b2[i] = (float)b2[i];
+        for (int j = 0; j < 6; j++) s->a[i][j] = (float)a[i][j];
+      }
+      s->adaptive = 1; s->errorder = 4.;
+      break;
+    }
+    case MMX_SOLVER_RKDP: {
+      s->stages = 7; s->fsal = 1;
+      double c[7] = {0., 1. / 5., 3. / 10., 4. / 5., 8. / 9., 1., 1.};
+      double a[7][7] = {{0}, {1. / 5.}, {3. / 40., 9. / 40.}, {44. / 45., -56. / 15., 32. / 9.},
+                        {19372. / 6561., -25360. / 2187., 64448. / 6561., -212. / 729.},
+                        {9017. / 3168., -355. / 33., 46732. / 5247., 49. / 176., -5103. / 18656.},
+                        {35. / 384., 0., 500. / 1113., 125. / 192., -2187. / 6784., 11. / 84.}};
+      double b[7] = {35. / 384., 0., 500. / 1113., 125. / 192., -2187. / 6784., 11. / 84., 0};
+      double b2[7] = {5179. / 57600., 0., 7571. / 16695., 393. / 640., -92097. / 339200., 187. / 2100., 1. / 40.};
+      for (int i = 0; i < 7; i++) {
+        s->c[i] = (float)c[i]; s->b[i] = (float)b[i]; s->b2[i] = (float)b2[i];
+        for (int j = 0; j < 7; j++) s->a[i][j] = (float)a[i][j];
+      }
+      s->adaptive = 1; s->errorder = 4.;
+      break;
+    }
+    default:
+      s->stages = 0;
+  }
+}
+
+// ------------------------------ launches ------------------------------
+static PassTimer* timer_for(mmx_solver* s, const char* name) {
+  for (auto& t : s->timers)
+    if (t.name == name) return &t;
+  s->timers.push_back(PassTimer());
+  s->timers.back().name = name;
+  return &s->timers.back();
+}
+
+struct ScopedPass {
+  mmx_solver* s;
+  cudaStream_t st;
+  PassTimer* t = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ScopedPass(mmx_solver* s_, const char* name, cudaStream_t st_) : s(s_), st(st_) {
+    if (!s->profile) return;
+    t = timer_for(s, name);
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, st);
+  }
+  ~ScopedPass() {
+    if (!t) return;
+    cudaEventRecord(b, st);
+    t->pending.push_back({a, b});
+    t->launches++;
+  }
+};
+
+static void flush_timers(mmx_solver* s) {
+  for (auto& t : s->timers) {
+    for (auto& pr : t.pending) {
+      cudaEventSynchronize(pr.second);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, pr.first, pr.second);
+      t.ms += ms;
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+    }
+    t.pending.clear();
+  }
+}
+
+static cudaError_t launch_xconv(mmx_solver* s, cudaStream_t st) {
+  int P0 = s->P[0];
+  int tk = 1;
+  while (tk < 32 && P0 * 3 * tk * 2 <= (is_pow2(P0) ? 4096 : 2048)) tk *= 2;
+  size_t smem = sizeof(float2) * (size_t)P0 * 3 * tk;
+  int ncol = s->P[1] * s->HZ;
+  ScopedPass sp(s, "xconv", st);
+  SHAPE_DISPATCH(P0 * 3 * tk, is_pow2(P0), {
+    allow_smem(k_xconv<T, E, P2>, smem);
+    k_xconv<T, E, P2><<<div_up(ncol, tk), T, smem, st>>>(s->S, s->bp.fx, s->K, s->N[0], s->P[1], s->HZ, s->CS, tk);
+  });
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_yconv2d(mmx_solver* s, cudaStream_t st) {
+  int P1 = s->P[1];
+  int tk = 1;
+  while (tk < 32 && P1 * 3 * tk * 2 <= (is_pow2(P1) ? 4096 : 2048) && tk * 2 <= s->HZ) tk *= 2;
+  size_t smem = sizeof(float2) * (size_t)P1 * 3 * tk;
+  ScopedPass sp(s, "yconv2d", st);
+  SHAPE_DISPATCH(P1 * 3 * tk, is_pow2(P1), {
+    allow_smem(k_yconv2d<T, E, P2>, smem);
+    k_yconv2d<T, E, P2><<<div_up(s->HZ, tk), T, smem, st>>>(s->S, s->bp.fy, s->K, s->N[1], s->HZ, s->CS, tk);
+  });
+  return cudaGetLastError();
+}
+
+template <int MODE>
+static cudaError_t launch_zinv(mmx_solver* s, const EpiArgs& ea, cudaStream_t st) {
+  int M = s->P[2] / 2;
+  int nrows = s->N[0] * s->N[1];
+  int rows = 1;
+  while (3 * (rows * 2) * (M + 1) <= (is_pow2(M) ? 4096 : 2048) && rows * 2 <= nrows) rows *= 2;
+  size_t smem = sizeof(float2) * (size_t)3 * rows * (M + 1);
+  ScopedPass sp(s, "zinv_epi", st);
+  SHAPE_DISPATCH(3 * rows * (M + 1), is_pow2(M), {
+    allow_smem(k_zinv_epi<T, E, P2, MODE>, smem);
+    k_zinv_epi<T, E, P2, MODE><<<div_up(nrows, rows), T, smem, st>>>(s->S, s->bp.fz, s->bp.twz, s->N[0], s->P[1],
+                                                                        s->HZ, s->CS, rows, nrows, ea);
+  });
+  return cudaGetLastError();
+}
+
+// forward part of the field evaluation: m -> S (after the kernel multiply)
+static cudaError_t conv_front(mmx_solver* s, const float* m, cudaStream_t st) {
+  cudaError_t e;
+  {
+    ZPass z = box_zpass(&s->bp, 3, s->N[0], s->n, s->CS);
+    ScopedPass sp(s, "zfwd", st);
+    e = launch_z_r2c(m, s->S, z, st);
+    if (e != cudaSuccess) return e;
+  }
+  if (s->is2d) return launch_yconv2d(s, st);
+  {
+    ColPass y;
+    y.f = s->bp.fy;
+    y.nplanes = 3 * s->N[0];
+    y.plane_stride = (int64_t)s->P[1] * s->HZ;
+    y.ncols = s->HZ;
+    y.stride_i = s->HZ;
+    y.n_in = s->N[1];
+    y.n_out = s->P[1];
+    y.inv = 0;
+    ScopedPass sp(s, "yfwd", st);
+    e = launch_col(s->S, s->S, y, st);
+    if (e != cudaSuccess) return e;
+  }
+  e = launch_xconv(s, st);
+  if (e != cudaSuccess) return e;
+  {
+    ColPass y;
+    y.f = s->bp.fy;
+    y.nplanes = 3 * s->N[0];
+    y.plane_stride = (int64_t)s->P[1] * s->HZ;
+    y.ncols = s->HZ;
+    y.stride_i = s->HZ;
+    y.n_in = s->P[1];
+    y.n_out = s->N[1];
+    y.inv = 1;
+    ScopedPass sp(s, "yinv", st);
+    e = launch_col(s->S, s->S, y, st);
+  }
+  return e;
+}
+
+static EpiArgs base_args(mmx_solver* s) {
+  EpiArgs ea;
+  memset(&ea, 0, sizeof(ea));
+  ea.N1 = s->N[1];
+  ea.N2 = s->N[2];
+  ea.n = s->n;
+  for (int d = 0; d < 3; d++) {
+    ea.lf.hext[d] = s->p.hext[d];
+    ea.lf.u[d] = s->p.anis_axis[d];
+  }
+  ea.lf.anis = s->p.anis_type;
+  ea.lf.K = s->p.anis_k;
+  ea.alpha = s->p.alpha;
+  return ea;
+}
+
+// ------------------------------ steps ---------------------------------
+// Host float32 arithmetic (one rounding per operation; x86-64 SSE, no
+// contraction) for the scalars the Go driver computes in float32.
+static inline float f32_div(float a, float b) { volatile float r = a / b; return r; }
+static inline float f32_mul(float a, float b) { volatile float r = a * b; return r; }
+static inline float f32_add(float a, float b) { volatile float r = a + b; return r; }
+static cudaError_t heun_step(mmx_solver* s, cudaStream_t st) {
+  // dtGilbert = dt / (1 + alpha^2)   (torque.go:49-51)
+  float dtg = f32_div(s->dt, f32_add(1.f, f32_mul(s->p.alpha, s->p.alpha)));
+  cudaError_t e;
+  EpiArgs ea = base_args(s);
+  ea.dtg = dtg;
+  // predictor
+  e = conv_front(s, s->m, st);
+  if (e != cudaSuccess) return e;
+  ea.m_in = s->m;
+  ea.out0 = s->t0;
+  ea.out1 = s->m1;
+  e = launch_zinv<EPI_HEUN1>(s, ea, st);
+  if (e != cudaSuccess) return e;
+  // corrector
+  e = conv_front(s, s->m1, st);
+  if (e != cudaSuccess) return e;
+  ea.m_in = s->m1;
+  ea.aux0 = s->t0;
+  ea.aux1 = s->m;
+  ea.out0 = s->m;
+  ea.out1 = nullptr;
+  ea.err = s->p.max_error != 0.f ? s->scratch : nullptr;
+  if (ea.err) {
+    e = cudaMemsetAsync(s->scratch, 0, sizeof(float), st);
+    if (e != cudaSuccess) return e;
+  }
+  return launch_zinv<EPI_HEUN2>(s, ea, st);
+}
+
+// RK stage i: combine the stage input, transform, torque epilogue.
+static cudaError_t rk_stage(mmx_solver* s, int i, cudaStream_t st, float* dt_dev) {
+  cudaError_t e;
+  const float* src = s->m;
+  ZComb cb;
+  memset(&cb, 0, sizeof(cb));
+  bool comb = false;
+  for (int j = 0; j < s->stages; j++)
+    if (s->a[i][j] != 0.f) comb = true;
+  ZPass z = box_zpass(&s->bp, 3, s->N[0], s->n, s->CS);
+  if (comb) {
+    cb.m0 = s->m;
+    for (int j = 0; j < s->stages; j++) { cb.k[j] = s->kb[j]; cb.a[j] = s->a[i][j]; }
+    cb.nk = s->stages;
+    cb.dt = dt_dev;
+    cb.out = s->m1;
+    src = s->m1;
+  }
+  {
+    ScopedPass sp(s, "zfwd", st);
+    e = launch_z_r2c(s->m, s->S, z, st, comb ? &cb : nullptr);
+    if (e != cudaSuccess) return e;
+  }
+  // remaining passes of the field evaluation
+  if (s->is2d) {
+    e = launch_yconv2d(s, st);
+  } else {
+    ColPass y;
+    y.f = s->bp.fy;
+    y.nplanes = 3 * s->N[0];
+    y.plane_stride = (int64_t)s->P[1] * s->HZ;
+    y.ncols = s->HZ;
+    y.stride_i = s->HZ;
+    y.n_in = s->N[1];
+    y.n_out = s->P[1];
+    y.inv = 0;
+    {
+      ScopedPass sp(s, "yfwd", st);
+      e = launch_col(s->S, s->S, y, st);
+    }
+    if (e != cudaSuccess) return e;
+    e = launch_xconv(s, st);
+    if (e != cudaSuccess) return e;
+    y.n_in = s->P[1];
+    y.n_out = s->N[1];
+    y.inv = 1;
+    {
+      ScopedPass sp(s, "yinv", st);
+      e = launch_col(s->S, s->S, y, st);
+    }
+  }
+  if (e != cudaSuccess) return e;
+  EpiArgs ea = base_args(s);
+  ea.dtg = f32_div(1.f, f32_add(1.f, f32_mul(s->p.alpha, s->p.alpha)));  // Torque = DeltaM(dt=1)
+  ea.m_in = src;
+  ea.dt_dev = dt_dev;
+  for (int j = 0; j < s->stages; j++) ea.kbuf[j] = s->kb[j];
+  ea.stage = i;
+  if (i == s->stages - 1) {
+    // last stage: k_last, then m_high (b) and, if adaptive, m_low (b2)
+    ea.out0 = s->kb[i];
+    ea.aux0 = s->m;
+    ea.out1 = s->mnew;
+    ea.rk.nk = s->stages;
+    for (int j = 0; j < s->stages; j++) { ea.rk.a[j] = s->b[j]; ea.rk.b2[j] = s->b2[j]; }
+    ea.rk.final_stage = 1;
+    ea.rk.adaptive = s->adaptive;
+    ea.err = s->adaptive ? s->scratch : nullptr;
+    return launch_zinv<EPI_RK>(s, ea, st);
+  }
+  ea.out0 = s->kb[i];
+  if (i == 0) ea.err = s->scratch + 1;  // max |k0|: the reference's 'torque'
+  return launch_zinv<EPI_TORQUE>(s, ea, st);
+}
+
+__global__ void k_finalize_accept(float* __restrict__ m, const float* __restrict__ mnew, int64_t n,
+                                  const int* __restrict__ accept) {
+  bool acc = *accept != 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float x, y, z;
+    if (acc) { x = mnew[i]; y = mnew[n + i]; z = mnew[2 * n + i]; }
+    else { x = m[i]; y = m[n + i]; z = m[2 * n + i]; }
+    llg_normalize(x, y, z);
+    m[i] = x;
+    m[n + i] = y;
+    m[2 * n + i] = z;
+  }
+}
+
+static int grid_1d(int64_t n) {
+  int64_t b = (n + 255) / 256;
+  int64_t cap = (int64_t)mmx_sm_count() * 8;
+  return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+}
+
+// RK.step (rk.go:279-445): up to 10 trials.  The stage kernels read dt
+// from device memory; the controller runs on the host in float32 exactly
+// as the Go code.  Fixed-step tableaux never read back; adaptive ones read
+// 8 bytes (error, maximum torque) per trial, the same synchronisation the
+// reference's two reductions per step impose.
+static int rk_step(mmx_solver* s, cudaStream_t st) {
+  float* dt_dev = s->scratch + 2;
+  int* acc_dev = reinterpret_cast<int*>(s->scratch + 3);
+  const int last = s->stages - 1;
+  const float ut = s->p.unit_time;
+  const bool bounds = s->p.min_dm != 0.f || s->p.max_dm != 0.f || s->p.min_dt != 0.f || s->p.max_dt != 0.f;
+  double time0 = s->time;
+  int good = 0, trials = 0;
+  while (!good && trials < 10) {
+    trials++;
+    for (int i = 0; i < s->stages; i++) {
+      if (s->fsal && i == 0 && s->fsal_init) {
+        // FSAL copy k0 <- k_last (rk.go:311-315), done as a buffer swap.
+        // The reference repeats it on a retry, so the retry starts from the
+        // rejected attempt's last torque; the clean mode keeps k0.
+        if (trials == 1 || s->p.faithful) {
+          float* t = s->kb[0];
+          s->kb[0] = s->kb[last];
+          s->kb[last] = t;
+        }
+        MMX_TRY(cudaMemsetAsync(s->scratch + 1, 0, sizeof(float), st));
+        k_maxabs<<<grid_1d(3 * s->n), 256, 0, st>>>(s->kb[0], 3 * s->n, s->scratch + 1);
+        MMX_TRY(cudaGetLastError());
+      } else {
+        if (i == 0) MMX_TRY(cudaMemsetAsync(s->scratch + 1, 0, sizeof(float), st));
+        if (i == last && s->adaptive) MMX_TRY(cudaMemsetAsync(s->scratch, 0, sizeof(float), st));
+        MMX_TRY(cudaMemcpyAsync(dt_dev, &s->dt, sizeof(float), cudaMemcpyHostToDevice, st));
+        cudaError_t e = rk_stage(s, i, st, dt_dev);
+        if (e != cudaSuccess) { mmx_set_error(cudaGetErrorString(e)); return MMX_ERR_CUDA; }
+        s->fsal_init = 1;
+      }
+      if (i == 0 && bounds) {
+        // dt bounds from the maximum torque (rk.go:348-373)
+        float mt = 0;
+        MMX_TRY(cudaMemcpyAsync(&mt, s->scratch + 1, sizeof(float), cudaMemcpyDeviceToHost, st));
+        MMX_TRY(cudaStreamSynchronize(st));
+        s->torque = mt;
+        float dm = f32_mul(s->dt, mt);
+        if (dm < s->p.min_dm) s->dt = f32_div(s->p.min_dm, mt);
+        if (f32_mul(s->dt, ut) < s->p.min_dt) s->dt = f32_div(s->p.min_dt, ut);
+        if (s->p.max_dm != 0.f && dm > s->p.max_dm) s->dt = f32_div(s->p.max_dm, mt);
+        if (s->p.max_dt != 0.f && f32_mul(s->dt, ut) > s->p.max_dt) s->dt = f32_div(s->p.max_dt, ut);
+        if (s->dt != s->dt) { mmx_set_error("dt = NaN"); return MMX_ERR_NAN; }
+      }
+    }
+    s->time = time0 + (double)s->dt;
+    if (!s->adaptive) {
+      good = 1;
+      int one = 1;
+      MMX_TRY(cudaMemcpyAsync(acc_dev, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+      break;
+    }
+    float sc[2];
+    MMX_TRY(cudaMemcpyAsync(sc, s->scratch, sizeof(float) * 2, cudaMemcpyDeviceToHost, st));
+    MMX_TRY(cudaStreamSynchronize(st));
+    float err = sc[0];
+    s->torque = sc[1];
+    s->step_error = err;
+    float factor = (float)pow((double)f32_div(s->p.max_error, err), 1. / s->errorder);
+    if (factor > 2.f) factor = 2.f;
+    if (factor < 0.01f) factor = 0.01f;
+    s->dt = f32_mul(s->dt, factor);
+    if (s->dt != s->dt || err != err) { mmx_set_error("dt = NaN"); return MMX_ERR_NAN; }
+    if (err > f32_mul(2.f, s->p.max_error)) {
+      good = 0;
+    } else {
+      good = 1;
+      if (f32_mul(s->dt, ut) < s->p.min_dt) s->dt = f32_div(s->p.min_dt, ut);
+      if (s->p.max_dt != 0.f && f32_mul(s->dt, ut) > s->p.max_dt) s->dt = f32_div(s->p.max_dt, ut);
+    }
+    int accv = good;
+    MMX_TRY(cudaMemcpyAsync(acc_dev, &accv, sizeof(int), cudaMemcpyHostToDevice, st));
+  }
+  // m <- normalize(m_high) if accepted, else normalize(m)   (rk.go:444)
+  k_finalize_accept<<<grid_1d(s->n), 256, 0, st>>>(s->m, s->mnew, s->n, acc_dev);
+  MMX_TRY(cudaGetLastError());
+  return MMX_OK;
+}
+
+static int heun_adaptive_update(mmx_solver* s, cudaStream_t st) {
+  float err = 0;
+  MMX_TRY(cudaMemcpyAsync(&err, s->scratch, sizeof(float), cudaMemcpyDeviceToHost, st));
+  MMX_TRY(cudaStreamSynchronize(st));
+  s->step_error = err;
+  float factor = f32_div(s->p.max_error, err);
+  if (factor > 2.f) factor = 2.f;
+  if (factor < 0.01f) factor = 0.01f;
+  s->dt = f32_mul(s->dt, factor);
+  return MMX_OK;
+}
+
+// ------------------------------ API -----------------------------------
+extern "C" int mmx_face_kernel6(const int P[3], const int periodic[3], const float cellsize[3], int accuracy,
+                                int exch6, float* k6, cudaStream_t stream) {
+  if (!P || !periodic || !cellsize || !k6 || accuracy <= 0) { mmx_set_error("bad argument"); return MMX_ERR_ARG; }
+  FaceKernelArgs a;
+  for (int d = 0; d < 3; d++) {
+    a.P[d] = P[d];
+    a.periodic[d] = periodic[d];
+    a.cs[d] = cellsize[d];
+    if (P[d] < 1) { mmx_set_error("bad size"); return MMX_ERR_SIZE; }
+  }
+  a.accuracy = accuracy;
+  // loop bounds of demag.go:136-154
+  for (int d = 0; d < 3; d++) {
+    int lo = -(P[d] - 1) / 2, hi = P[d] / 2 - 1;
+    if (d == 0 && P[0] == 1 && periodic[0] == 0) hi = 0;
+    lo *= periodic[d] + 1;
+    hi *= periodic[d] + 1;
+    a.lo[d] = lo;
+    a.hi[d] = hi;
+  }
+  int64_t n3 = (int64_t)P[0] * P[1] * P[2];
+  int blocks = (int)((n3 + 127) / 128);
+  int cap = mmx_sm_count() * 16;
+  if (blocks > cap) blocks = cap;
+  k_face_kernel6<<<blocks, 128, 0, stream>>>(k6, a);
+  MMX_TRY(cudaGetLastError());
+  if (exch6) {
+    k_add_exch6<<<1, 1, 0, stream>>>(k6, P[0], P[1], P[2], cellsize[0], cellsize[1], cellsize[2]);
+    MMX_TRY(cudaGetLastError());
+  }
+  return MMX_OK;
+}
+
+static void solver_free(mmx_solver* s) {
+  if (!s) return;
+  if (s->gexec) cudaGraphExecDestroy(s->gexec);
+  cudaFree(s->S);
+  cudaFree(s->kh);
+  cudaFree(s->m);
+  cudaFree(s->t0);
+  cudaFree(s->m1);
+  cudaFree(s->mnew);
+  cudaFree(s->scratch);
+  for (int i = 0; i < RK_MAXS; i++) cudaFree(s->kb[i]);
+  for (auto& t : s->timers)
+    for (auto& pr : t.pending) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+  delete s;
+}
+
+extern "C" int mmx_solver_create(const mmx_params* p, mmx_solver** out) {
+  if (!p || !out) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  *out = nullptr;
+  mmx_solver* s = new mmx_solver();
+  s->p = *p;
+  if (s->p.accuracy <= 0) s->p.accuracy = 8;
+  for (int d = 0; d < 3; d++) {
+    s->N[d] = p->size[d];
+    if (s->N[d] < 1) { delete s; mmx_set_error("size must be >= 1"); return MMX_ERR_SIZE; }
+    s->P[d] = (s->N[d] > 1 && p->periodic[d] == 0) ? 2 * s->N[d] : s->N[d];
+  }
+  if (s->N[2] < 2 || s->N[1] < 2) {
+    delete s;
+    mmx_set_error("internal Y and Z sizes must be >= 2 (gpu_fft0.cu:124-126)");
+    return MMX_ERR_SIZE;
+  }
+  s->is2d = s->P[0] == 1;
+  s->n = (int64_t)s->N[0] * s->N[1] * s->N[2];
+  int rc = box_plan_init(&s->bp, s->N, s->P);
+  if (rc != MMX_OK) { delete s; mmx_set_error("unsupported padded size (radices 2,3,5,7; <= 16384)"); return rc; }
+  s->HZ = s->bp.HZ;
+  s->CS = (int64_t)s->N[0] * s->P[1] * s->HZ;
+  set_tableau(s);
+  if (p->solver != MMX_SOLVER_HEUN && s->stages == 0) { delete s; mmx_set_error("unknown solver"); return MMX_ERR_ARG; }
+  s->dt = p->dt;
+  size_t n3 = 3 * (size_t)s->n;
+#define ALLOC(ptr, bytes)                                                   \
+  if (cudaMalloc(&(ptr), (bytes)) != cudaSuccess) {                         \
+    solver_free(s);                                                         \
+    mmx_set_error("out of device memory");                                  \
+    return MMX_ERR_MEM;                                                     \
+  }
+  ALLOC(s->S, sizeof(float2) * 3 * (size_t)s->CS);
+  ALLOC(s->m, sizeof(float) * n3);
+  ALLOC(s->m1, sizeof(float) * n3);
+  ALLOC(s->scratch, sizeof(float) * 16);
+  cudaMemset(s->m, 0, sizeof(float) * n3);
+  cudaMemset(s->scratch, 0, sizeof(float) * 16);
+  if (p->solver == MMX_SOLVER_HEUN) {
+    ALLOC(s->t0, sizeof(float) * n3);
+  } else {
+    for (int i = 0; i < s->stages; i++) ALLOC(s->kb[i], sizeof(float) * n3);
+    ALLOC(s->mnew, sizeof(float) * n3);
+  }
+  // kernel: real space on the GPU, transformed component by component
+  {
+    int64_t p3 = (int64_t)s->P[0] * s->P[1] * s->P[2];
+    float* k6 = nullptr;
+    float2* spec = nullptr;
+    int O0 = s->P[0] / 2 + 1, O1 = s->P[1] / 2 + 1;
+    int64_t ocs = (int64_t)O0 * O1 * s->HZ;
+    ALLOC(s->kh, sizeof(float) * 6 * ocs);
+    if (cudaMalloc(&k6, sizeof(float) * 6 * p3) != cudaSuccess ||
+        cudaMalloc(&spec, sizeof(float2) * (size_t)s->P[0] * s->P[1] * s->HZ) != cudaSuccess) {
+      cudaFree(k6);
+      solver_free(s);
+      mmx_set_error("out of device memory (kernel build)");
+      return MMX_ERR_MEM;
+    }
+    float cs[3] = {p->cellsize[0], p->cellsize[1], p->cellsize[2]};
+    rc = mmx_face_kernel6(s->P, p->periodic, cs, s->p.accuracy, p->exch_type == 6, k6, 0);
+    BoxPlan full;
+    if (rc == MMX_OK) rc = box_plan_init(&full, s->P, s->P);
+    // loadKernel6 (conv.go:126-160): same transform, real part x 1/N
+    float norm = f32_div(1.f, (float)p3);
+    for (int c = 0; c < 6 && rc == MMX_OK; c++) {
+      if (s->is2d && (c == 4 || c == 5)) {
+        cudaMemset(s->kh + c * ocs, 0, sizeof(float) * ocs);
+        continue;
+      }
+      if (box_forward(&full, k6 + c * p3, spec, 0) != cudaSuccess) rc = MMX_ERR_CUDA;
+      k_extract_octant<<<grid_1d(ocs), 256>>>(spec, s->kh + c * ocs, O0, O1, s->P[1], s->HZ, norm);
+    }
+    cudaError_t ce = cudaDeviceSynchronize();
+    cudaFree(k6);
+    cudaFree(spec);
+    if (rc != MMX_OK || ce != cudaSuccess) {
+      solver_free(s);
+      mmx_set_error(ce != cudaSuccess ? cudaGetErrorString(ce) : "kernel build failed");
+      return rc != MMX_OK ? rc : MMX_ERR_CUDA;
+    }
+    s->K.kh = s->kh;
+    s->K.O0 = O0;
+    s->K.O1 = O1;
+    s->K.HZ = s->HZ;
+    s->K.P0 = s->P[0];
+    s->K.P1 = s->P[1];
+    s->K.cs = ocs;
+  }
+#undef ALLOC
+  *out = s;
+  return MMX_OK;
+}
+
+extern "C" int mmx_solver_destroy(mmx_solver* s) {
+  solver_free(s);
+  return MMX_OK;
+}
+
+extern "C" int mmx_solver_set_m(mmx_solver* s, const float* m, int on_host, cudaStream_t st) {
+  if (!s || !m) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  MMX_TRY(cudaMemcpyAsync(s->m, m, sizeof(float) * 3 * s->n, on_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
+  MMX_TRY(cudaStreamSynchronize(st));
+  s->fsal_init = 0;
+  return MMX_OK;
+}
+
+extern "C" int mmx_solver_get_m(mmx_solver* s, float* m, int on_host, cudaStream_t st) {
+  if (!s || !m) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  MMX_TRY(cudaMemcpyAsync(m, s->m, sizeof(float) * 3 * s->n, on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st));
+  MMX_TRY(cudaStreamSynchronize(st));
+  return MMX_OK;
+}
+
+extern "C" int mmx_solver_normalize(mmx_solver* s, cudaStream_t st) {
+  if (!s) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  k_normalize3<<<grid_1d(s->n), 256, 0, st>>>(s->m, s->n);
+  MMX_TRY(cudaGetLastError());
+  return MMX_OK;
+}
+
+extern "C" int mmx_solver_field(mmx_solver* s, const float* m, float* h, cudaStream_t st) {
+  if (!s || !m || !h) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  cudaError_t e = conv_front(s, m, st);
+  if (e == cudaSuccess) {
+    EpiArgs ea = base_args(s);
+    ea.m_in = m;
+    ea.out0 = h;
+    e = launch_zinv<EPI_FIELD>(s, ea, st);
+  }
+  if (e != cudaSuccess) { mmx_set_error(cudaGetErrorString(e)); return MMX_ERR_CUDA; }
+  return MMX_OK;
+}
+
+static int step_once(mmx_solver* s, cudaStream_t st) {
+  if (s->p.solver == MMX_SOLVER_HEUN) {
+    cudaError_t e = heun_step(s, st);
+    if (e != cudaSuccess) { mmx_set_error(cudaGetErrorString(e)); return MMX_ERR_CUDA; }
+    s->time += (double)s->dt;
+    if (s->p.max_error != 0.f) return heun_adaptive_update(s, st);
+    return MMX_OK;
+  }
+  return rk_step(s, st);
+}
+
+extern "C" int mmx_solver_step(mmx_solver* s, int nsteps, cudaStream_t st) {
+  if (!s || nsteps < 0) { mmx_set_error("bad argument"); return MMX_ERR_ARG; }
+  bool graphable = s->use_graph && !s->profile && s->p.solver == MMX_SOLVER_HEUN && s->p.max_error == 0.f;
+  for (int k = 0; k < nsteps; k++) {
+    if (graphable) {
+      if (!s->gexec || s->gstream != st) {
+        if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+        cudaStream_t cap = st;
+        bool own = false;
+        if (cap == 0) { MMX_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)); own = true; }
+        cudaGraph_t g;
+        MMX_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = heun_step(s, cap);
+        cudaError_t e2 = cudaStreamEndCapture(cap, &g);
+        if (own) cudaStreamDestroy(cap);
+        if (e != cudaSuccess || e2 != cudaSuccess) { mmx_set_error("graph capture failed"); return MMX_ERR_CUDA; }
+        MMX_TRY(cudaGraphInstantiate(&s->gexec, g, 0));
+        cudaGraphDestroy(g);
+        s->gstream = st;
+      }
+      MMX_TRY(cudaGraphLaunch(s->gexec, st));
+      s->time += (double)s->dt;
+    } else {
+      int rc = step_once(s, st);
+      if (rc != MMX_OK) return rc;
+    }
+    s->steps++;
+  }
+  if (s->profile) flush_timers(s);
+  return MMX_OK;
+}
+
+extern "C" int mmx_solver_state(mmx_solver* s, double* time, float* dt, float* max_torque, float* step_error,
+                                long long* steps) {
+  if (!s) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  if (time) *time = s->time;
+  if (dt) *dt = s->dt;
+  if (max_torque) *max_torque = s->torque;
+  if (step_error) *step_error = s->step_error;
+  if (steps) *steps = s->steps;
+  return MMX_OK;
+}
+
+extern "C" int mmx_solver_set_hext(mmx_solver* s, const float hext[3]) {
+  if (!s || !hext) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  for (int d = 0; d < 3; d++) s->p.hext[d] = hext[d];
+  if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+  return MMX_OK;
+}
+
+extern "C" float* mmx_solver_m_device(mmx_solver* s) { return s ? s->m : nullptr; }
+
+extern "C" int mmx_solver_use_graph(mmx_solver* s, int on) {
+  if (!s) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  s->use_graph = on;
+  if (!on && s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+  return MMX_OK;
+}
+
+extern "C" int mmx_solver_profile(mmx_solver* s, int on) {
+  if (!s) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  if (s->profile) flush_timers(s);
+  s->profile = on;
+  if (on) s->timers.clear();
+  return MMX_OK;
+}
+
+extern "C" int mmx_solver_pass_times(mmx_solver* s, int max, char (*names)[32], double* ms, long long* launches,
+                                     int* n) {
+  if (!s || !n) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  flush_timers(s);
+  int k = 0;
+  for (auto& t : s->timers) {
+    if (k >= max) break;
+    if (names) { strncpy(names[k], t.name.c_str(), 31); names[k][31] = 0; }
+    if (ms) ms[k] = t.ms;
+    if (launches) launches[k] = t.launches;
+    k++;
+  }
+  *n = k;
+  return MMX_OK;
+}

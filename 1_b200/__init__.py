@@ -180,6 +180,7 @@ MMX = {
     "mmx_solver_normalize": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "mmx_solver_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "mmx_solver_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "mmx_solver_avg_m": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "mmx_solver_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                         ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
                                         ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_longlong)]),
@@ -346,6 +347,17 @@ class Solver:
 
     def field(self, m_ptr, h_ptr, stream=None):
         _check(lib().mmx_solver_field(self.h, m_ptr, h_ptr, stream))
+
+    def avg_m(self, out_ptr=None, on_host=True, stream=None):
+        """<m> per internal component; into out_ptr (host or device) or a
+        new numpy array (synchronous)."""
+        if out_ptr is None:
+            out = np.zeros(3, np.float32)
+            _check(lib().mmx_solver_avg_m(self.h, out.ctypes.data, 1, stream))
+            import torch
+            torch.cuda.synchronize()
+            return out
+        _check(lib().mmx_solver_avg_m(self.h, out_ptr, 1 if on_host else 0, stream))
 
     def state(self):
         t, dt, tq, er, st = ctypes.c_double(), ctypes.c_float(), ctypes.c_float(), ctypes.c_float(), ctypes.c_longlong()

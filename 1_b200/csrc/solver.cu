@@ -788,6 +788,35 @@ __global__ void k_finalize_accept(float* __restrict__ m, const float* __restrict
   }
 }
 
+// <m>: per-component sums in float64 (block reduction + one atomic per
+// block), divided by the cell count (simoutput.go:236, simget.go:32).
+__global__ void k_sum3(const float* __restrict__ m, int64_t n, double* __restrict__ acc) {
+  __shared__ double sh[3][32];
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    v[0] += m[i];
+    v[1] += m[n + i];
+    v[2] += m[2 * n + i];
+  }
+  for (int c = 0; c < 3; c++)
+    for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0)
+    for (int c = 0; c < 3; c++) sh[c][w] = v[c];
+  __syncthreads();
+  if (w == 0) {
+    int nw = blockDim.x >> 5;
+    for (int c = 0; c < 3; c++) {
+      double t = l < nw ? sh[c][l] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (l == 0) atomicAdd(&acc[c], t);
+    }
+  }
+}
+__global__ void k_avg_finish(const double* __restrict__ acc, double n, float* __restrict__ out) {
+  if (threadIdx.x < 3) out[threadIdx.x] = (float)(acc[threadIdx.x] / n);
+}
+
 static int grid_1d(int64_t n) {
   int64_t b = (n + 255) / 256;
   int64_t cap = (int64_t)mmx_sm_count() * 8;
@@ -1114,6 +1143,19 @@ extern "C" int mmx_solver_step(mmx_solver* s, int nsteps, cudaStream_t st) {
     s->steps++;
   }
   if (s->profile) flush_timers(s);
+  return MMX_OK;
+}
+
+extern "C" int mmx_solver_avg_m(mmx_solver* s, float* out3, int on_host, cudaStream_t st) {
+  if (!s || !out3) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  double* acc = reinterpret_cast<double*>(s->scratch + 8);
+  float* res = s->scratch + 4;
+  MMX_TRY(cudaMemsetAsync(acc, 0, 3 * sizeof(double), st));
+  k_sum3<<<grid_1d(s->n), 256, 0, st>>>(s->m, s->n, acc);
+  MMX_TRY(cudaGetLastError());
+  k_avg_finish<<<1, 32, 0, st>>>(acc, (double)s->n, on_host ? res : out3);
+  MMX_TRY(cudaGetLastError());
+  if (on_host) MMX_TRY(cudaMemcpyAsync(out3, res, 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
   return MMX_OK;
 }
 

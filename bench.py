@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Benchmark of the LLG time-stepping hot path on B200.
+
+Workload (default): the plain FP32 method on a single 3D grid of
+256 x 256 x 32 cells of 4 x 4 x 4 nm, Ms = 1.1e6 A/m, Aex = 1.5e-11 J/m,
+uniaxial Ku = 5e5 J/m^3 along z, alpha = 0.5, m = independent unit vectors
+uniform on the sphere (seed 2), zero field, Heun with a fixed dt = 1e-14 s.
+A step is one Heun step (two effective-field evaluations) of the whole grid.
+
+Prints one JSON line (rank 0).  Metric: cell-steps/s, whole job.
+  --impl ours       the fused B200 engine (mmx_* C ABI)
+  --impl reference  the reference's path on the host cores: MuMax 1 has no
+                    CPU implementation, so this is the CPU restatement of its
+                    algorithm (oracle/, FP32, OpenMP over all host threads)
+Multi-GPU: one process per GPU, each advancing its own replica of the grid
+(the single-grid path does not shard); value = all ranks' cell-steps / the
+slowest rank's time.
+"""
+import argparse
+import ctypes
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "plain-fp32-heun-256x256x32": dict(
+        grid=(256, 256, 32), cell=(4e-9, 4e-9, 4e-9), msat=1.1e6, aexch=1.5e-11, alpha=0.5, anis=1, k1=5e5,
+        axis=(0, 0, 1), solver="heun", dt=1e-14, seed=2, init="random"),
+    "plain-fp32-heun-128x32x1": dict(
+        grid=(128, 32, 1), cell=(3.90625e-9, 3.90625e-9, 3e-9), msat=8.0e5, aexch=1.3e-11, alpha=0.02,
+        bext=(-24.6e-3, 4.3e-3, 0.0), solver="heun", dt=1e-14, seed=1, init="tilted"),
+}
+DEFAULT = "plain-fp32-heun-256x256x32"
+
+
+def sim_kwargs(w):
+    keys = ("grid", "cell", "msat", "aexch", "alpha", "bext", "anis", "k1", "axis", "solver", "dt")
+    return {k: w[k] for k in keys if k in w}
+
+
+def seeded_m(grid, seed, mode):
+    """Internal [3][X][Y][Z] magnetisation: user components (x,y,z) drawn as
+    default_rng(seed).standard_normal((3, nz, ny, nx)); internal component C
+    is user component 2-C."""
+    nx, ny, nz = grid
+    u = np.random.default_rng(seed).standard_normal((3, nz, ny, nx))
+    v = 1.0 + 0.01 * u if mode == "tilted" else u
+    v = v / np.sqrt((v * v).sum(axis=0, keepdims=True))
+    return np.ascontiguousarray(v[::-1]).astype(np.float32)
+
+
+def pass_bytes(w):
+    """Algorithmic HBM bytes per launch of each kernel of one field
+    evaluation of the zero-aware padded convolution, and per cell-step for
+    Heun (two evaluations plus the predictor/corrector state).
+
+    3D: zfwd (read m, write Z spectra of the data rows), yfwd, xconv (X
+    transform + kernel multiply + inverse, reads the kernel octant), yinv,
+    zinv_epi (read Z spectra, Heun state in/out).  2D: zfwd, yconv2d,
+    zinv_epi."""
+    nx, ny, nz = w["grid"]
+    N0, N1, N2 = nz, ny, nx
+    P0 = 2 * N0 if N0 > 1 else 1
+    P1, P2 = 2 * N1, 2 * N2
+    HZ = P2 // 2 + 1
+    n = N0 * N1 * N2
+    zspec = 3 * N0 * N1 * HZ * 8      # Z-transformed data rows
+    yspec = 3 * N0 * P1 * HZ * 8      # after the Y transform
+    heun_epi = (36 + 48) * n // 2     # mean of predictor and corrector state traffic
+    if P0 > 1:
+        koct = 6 * (P0 // 2 + 1) * (P1 // 2 + 1) * HZ * 4
+        b = {"zfwd": 3 * n * 4 + zspec, "yfwd": zspec + yspec, "xconv": 2 * yspec + koct,
+             "yinv": yspec + zspec, "zinv_epi": zspec + heun_epi}
+    else:
+        koct = 4 * (P1 // 2 + 1) * HZ * 4
+        b = {"zfwd": 3 * n * 4 + zspec, "yconv2d": 2 * zspec + koct, "zinv_epi": zspec + heun_epi}
+    per_step = 2 * sum(b.values())
+    state = 9 * n * 4 + (yspec if P0 > 1 else zspec) + koct
+    return b, per_step / n, state
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a run."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                       "-lms", "100", "-i", str(device)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.f.read().splitlines():
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel, workload):
+    """Per-launch DRAM bytes of 'kernel' from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return d.get(workload, {}).get(kernel)
+
+
+def cpu_baseline(w, steps_budget_s=20.0):
+    """The CPU restatement of the reference's algorithm (oracle, FP32,
+    OpenMP over all host threads) on the same workload: bounded sample of
+    whole-grid steps after one untimed step."""
+    import oracle as O
+    kw = sim_kwargs(w)
+    cfg = O.make_cfg(**kw)
+    m = seeded_m(w["grid"], w["seed"], w["init"])
+    t0 = time.perf_counter()
+    o = O.OracleSim(cfg, m, bits=32)
+    setup = time.perf_counter() - t0
+    o.steps(1)
+    n = int(np.prod(w["grid"]))
+    done, t0 = 0, time.perf_counter()
+    while True:
+        o.steps(1)
+        done += 1
+        el = time.perf_counter() - t0
+        if el > steps_budget_s or done >= 50:
+            break
+    return {"value": n * done / el, "unit": "cell-steps/s", "cores": O.num_threads(), "kind": "port",
+            "sample": "%d whole-grid Heun steps of %s after 1 untimed step (setup incl. kernel %.1f s untimed)" % (
+                done, "x".join(map(str, w["grid"])), setup)}
+
+
+def run_reference(args, w, name):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cb = cpu_baseline(w)
+    line = {"metric": "cell-steps/s", "value": cb["value"], "unit": "cell-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * np.prod(w["grid"]) / cb["value"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": name, "grid": list(w["grid"]), "solver": w["solver"], "dt_s": w["dt"],
+                       "parallelism": "host threads (rank 0)"},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, w, name):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    eng = importlib.import_module("1_b200")
+    kw = sim_kwargs(w)
+    n = int(np.prod(w["grid"]))
+    m0 = seeded_m(w["grid"], w["seed"], w["init"])
+    s = eng.Solver(eng.mmx_params(**kw))
+    stream = torch.cuda.Stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-resident timed region (graph replay per step) ----
+    s.set_m(m0, sh)
+    s.normalize(sh)
+    s.use_graph(True)
+    s.step(args.warmup, sh)
+    barrier()
+    clocks = Clocks(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    ev0.record(stream)
+    s.step(args.steps, sh)
+    ev1.record(stream)
+    ev1.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    value = world * n * args.steps / (ms / 1e3)
+
+    # ---- per-kernel durations with CUDA events on the step's stream ----
+    s.use_graph(False)
+    s.profile(True)
+    ksteps = min(args.steps, 200)
+    s.step(ksteps, sh)
+    torch.cuda.synchronize()
+    times = s.pass_times()
+    s.profile(False)
+    barrier()
+
+    # ---- end to end through the C ABI with host buffers ----
+    s.use_graph(True)
+    pin_in = torch.from_numpy(m0.reshape(-1)).pin_memory()
+    pin_out = torch.empty(3 * n, dtype=torch.float32).pin_memory()
+    pin_avg = torch.empty((args.steps, 3), dtype=torch.float32).pin_memory()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    eng.lib().mmx_solver_set_m(s.h, ctypes.c_void_p(pin_in.data_ptr()), 1, sh)
+    s.normalize(sh)
+    row = pin_avg.data_ptr()
+    for k in range(args.steps):
+        s.step(1, sh)
+        s.avg_m(ctypes.c_void_p(row + 12 * k), True, sh)
+    eng.lib().mmx_solver_get_m(s.h, ctypes.c_void_p(pin_out.data_ptr()), 1, sh)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    ems = e0.elapsed_time(e1)
+    t = torch.tensor([ems], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ems = float(t.item())
+    e2e = world * n * args.steps / (ems / 1e3)
+    avg_last = pin_avg[-1].tolist()
+    s.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    b, bytes_per_cell_step, state = pass_bytes(w)
+    peak, peak_kind = measured_peaks()
+    dom = max(times, key=lambda k: times[k][0])
+    dom_ms = times[dom][0] / times[dom][1]
+    achieved = b[dom] / (dom_ms / 1e3) / 1e9
+    traffic = ncu_traffic(dom, name)
+    launches_per_step = sum(la for _, la in times.values()) / ksteps
+    line = {
+        "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": name, "grid": list(w["grid"]), "cell_m": list(w["cell"]), "solver": w["solver"],
+                   "dt_s": w["dt"], "parallelism": "replicas x%d" % world,
+                   "l2": "working set %.0f MB per GPU vs 126 MB L2 (no flush between steps)" % (state / 1e6)},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": b[dom], "avg_launch_ms": dom_ms,
+                     "step_bytes_per_cell": bytes_per_cell_step,
+                     "step_frac": bytes_per_cell_step * value / world / 1e9 / peak,
+                     "passes_ms_per_launch": {k: v[0] / v[1] for k, v in times.items()}},
+        "e2e": {"value": e2e, "unit": "cell-steps/s",
+                "h2d_bytes_per_step": 3 * n * 4 / args.steps,
+                "d2h_bytes_per_step": 12 + 3 * n * 4 / args.steps,
+                "path": "mmx C ABI: m from pinned host, per-step <m> to pinned host, final m to host",
+                "avg_m_last": avg_last},
+        "gpu_launches": int(round(launches_per_step * args.steps)),
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(w)
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, w, args.workload)
+    else:
+        run_ours(args, w, args.workload)
+
+
+if __name__ == "__main__":
+    main()

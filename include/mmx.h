@@ -91,6 +91,13 @@ int mmx_solver_step(mmx_solver* s, int nsteps, cudaStream_t stream);
  * array m (field.go:427-433); m and h are device arrays of 3*N floats. */
 int mmx_solver_field(mmx_solver* s, const float* m, float* h, cudaStream_t stream);
 
+/* <m>: the average magnetisation per internal component (the table output
+ * of src/go/sim/simoutput.go:236), summed in float64 on the device.  With
+ * on_host != 0, out3 is a host pointer filled by an asynchronous copy on
+ * 'stream' (pinned memory makes it truly asynchronous); else a device
+ * pointer. */
+int mmx_solver_avg_m(mmx_solver* s, float* out3, int on_host, cudaStream_t stream);
+
 /* Solver scalars: simulated time (internal units), current dt, the last
  * maximum torque and the last error estimate, steps taken. */
 int mmx_solver_state(mmx_solver* s, double* time, float* dt, float* max_torque, float* step_error, long long* steps);

@@ -191,6 +191,8 @@ MMX = {
     "mmx_solver_pass_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                              ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
                                              ctypes.POINTER(ctypes.c_int)]),
+    "mmx_reduce_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                         ctypes.c_void_p]),
     "mmx_face_kernel6": (ctypes.c_int, [c_int_p, c_int_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int,
                                         ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
 }

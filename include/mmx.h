@@ -115,6 +115,23 @@ int mmx_solver_use_graph(mmx_solver* s, int on);
 int mmx_solver_profile(mmx_solver* s, int on);
 int mmx_solver_pass_times(mmx_solver* s, int max, char (*names)[32], double* ms, long long* launches, int* n);
 
+/* Allocation-free reduction.  No counterpart in the reference: a variant of
+ * gpu_reduce (same operations, 1 add, 2 max, 3 max |x|, 4 min, 5 sum |x|)
+ * for callers that cannot call cudaMalloc -- code running while a CUDA
+ * graph is captured in global mode, host callbacks, or embedders that
+ * budget all device memory up front.  gpu_reduce allocates its partial
+ * sums on its first call; this one keeps them in an 8 KB array compiled
+ * into the library (held by every GPU that loads it until exit) and
+ * allocates nothing.  'input' (n floats) and 'result' (1 float) are device
+ * pointers; the launch is asynchronous on 'stream'.  n is limited to
+ * MMX_REDUCE_STATIC_MAX_N; larger n returns MMX_ERR_SIZE.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress)
+ * and should come before any stream capture.  Every call shares the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
+#define MMX_REDUCE_STATIC_BLOCKS 1024
+#define MMX_REDUCE_STATIC_MAX_N (MMX_REDUCE_STATIC_BLOCKS * 4096)
+int mmx_reduce_static(int operation, const float* input, int n, float* result, cudaStream_t stream);
+
 /* FaceKernel6 on the GPU: the 6 real-space components (XX,YY,ZZ,YZ,XZ,XY)
  * of the padded grid P, written to k6 (device, 6*P0*P1*P2 floats),
  * bit-identical to src/go/sim/demag.go:127-185 in float32.  If exch6 != 0

@@ -1,0 +1,139 @@
+// Per-cell epilogues of the inverse-Z pass: local fields, LLG torque and
+// the solver stage update, shared by the generic and the fixed-size
+// kernels.  Every operation is an explicitly rounded float32 operation in
+// the reference's order (see llg_ops.cuh).
+#pragma once
+#include "llg_ops.cuh"
+
+enum { EPI_FIELD = 0, EPI_HEUN1 = 1, EPI_HEUN2 = 2, EPI_TORQUE = 3, EPI_RK = 4 };
+
+#define RK_MAXS 7
+struct RKCoef {
+  float a[RK_MAXS];   // row a[i+1][0..i] (next stage input), or b for the final stage
+  float b2[RK_MAXS];  // lower-order weights (final stage, adaptive)
+  int nk;             // number of k's combined
+  int final_stage;    // 1: produce m_high / m_low / error
+  int adaptive;
+};
+
+struct EpiArgs {
+  int N1, N2;
+  int64_t n;            // cells per component
+  LocalField lf;
+  float alpha, dtg;
+  const float* m_in;    // magnetisation at which the field was evaluated
+  float* out0;
+  float* out1;
+  const float* aux0;
+  const float* aux1;
+  float* err;           // device scalar (maxabs target), may be null
+  const float* dt_dev;  // RK: device dt
+  float* kbuf[RK_MAXS]; // RK: stage torques
+  int stage;            // RK: index of this stage's k
+  RKCoef rk;
+};
+
+
+// cell g (index into one component), field (hx,hy,hz) from the convolution
+template <int MODE>
+__device__ __forceinline__ void epi_cell(const EpiArgs& ea, int64_t g, float hx, float hy, float hz, float& lmax) {
+    const int64_t n = ea.n;
+    float mx = ea.m_in[g], my = ea.m_in[n + g], mz = ea.m_in[2 * n + g];
+    llg_local(ea.lf, mx, my, mz, hx, hy, hz);
+    if (MODE == EPI_FIELD) {
+      ea.out0[g] = hx;
+      ea.out0[n + g] = hy;
+      ea.out0[2 * n + g] = hz;
+      return;
+    }
+    llg_delta_m(mx, my, mz, hx, hy, hz, ea.alpha, ea.dtg);
+    if (MODE == EPI_TORQUE) {
+      ea.out0[g] = hx;
+      ea.out0[n + g] = hy;
+      ea.out0[2 * n + g] = hz;
+      if (ea.err) lmax = fmaxf(lmax, fmaxf(fabsf(hx), fmaxf(fabsf(hy), fabsf(hz))));
+    } else if (MODE == EPI_HEUN1) {
+      // t0 = torque*dt; m1est = normalize(m + t0)   (adaptive_heun.go:141-146)
+      ea.out0[g] = hx;
+      ea.out0[n + g] = hy;
+      ea.out0[2 * n + g] = hz;
+      float ex = FA(mx, hx), ey = FA(my, hy), ez = FA(mz, hz);
+      llg_normalize(ex, ey, ez);
+      ea.out1[g] = ex;
+      ea.out1[n + g] = ey;
+      ea.out1[2 * n + g] = ez;
+    } else if (MODE == EPI_HEUN2) {
+      // t = 0.5 t1 + 0.5 t0; m = normalize(m + t)   (adaptive_heun.go:148-154)
+      float tx = FA(FM(0.5f, hx), FM(0.5f, ea.aux0[g]));
+      float ty = FA(FM(0.5f, hy), FM(0.5f, ea.aux0[n + g]));
+      float tz = FA(FM(0.5f, hz), FM(0.5f, ea.aux0[2 * n + g]));
+      float nx = FA(ea.aux1[g], tx), ny = FA(ea.aux1[n + g], ty), nz = FA(ea.aux1[2 * n + g], tz);
+      llg_normalize(nx, ny, nz);
+      ea.out0[g] = nx;
+      ea.out0[n + g] = ny;
+      ea.out0[2 * n + g] = nz;
+      if (ea.err) {
+        // error = maxabs(m1est - m)   (adaptive_heun.go:158-160)
+        float d0 = fabsf(FA(mx, FM(-1.f, nx)));
+        float d1 = fabsf(FA(my, FM(-1.f, ny)));
+        float d2 = fabsf(FA(mz, FM(-1.f, nz)));
+        lmax = fmaxf(lmax, fmaxf(d0, fmaxf(d1, d2)));
+      }
+    } else if (MODE == EPI_RK) {
+      float kx = hx, ky = hy, kz = hz;
+      float* kd = ea.out0;
+      kd[g] = kx;
+      kd[n + g] = ky;
+      kd[2 * n + g] = kz;
+      const float dt = *ea.dt_dev;
+      const float* m0 = ea.aux0;  // step start magnetisation
+      float q[3] = {m0[g], m0[n + g], m0[2 * n + g]};
+      // next stage input (or m_high): m0 + sum_j (dt a_j) k_j, j in order
+#pragma unroll
+      for (int j = 0; j < RK_MAXS; j++) {
+        if (j >= ea.rk.nk) break;
+        float a = ea.rk.a[j];
+        if (a == 0.f) continue;
+        float c = FM(dt, a);
+        float k0, k1, k2;
+        if (j == ea.stage) { k0 = kx; k1 = ky; k2 = kz; }
+        else { k0 = ea.kbuf[j][g]; k1 = ea.kbuf[j][n + g]; k2 = ea.kbuf[j][2 * n + g]; }
+        q[0] = FA(q[0], FM(c, k0));
+        q[1] = FA(q[1], FM(c, k1));
+        q[2] = FA(q[2], FM(c, k2));
+      }
+      if (ea.rk.final_stage && ea.rk.adaptive) {
+        float lo[3] = {m0[g], m0[n + g], m0[2 * n + g]};
+#pragma unroll
+        for (int j = 0; j < RK_MAXS; j++) {
+          if (j >= ea.rk.nk) break;
+          float b = ea.rk.b2[j];
+          if (b == 0.f) continue;
+          float c = FM(b, dt);
+          float k0, k1, k2;
+          if (j == ea.stage) { k0 = kx; k1 = ky; k2 = kz; }
+          else { k0 = ea.kbuf[j][g]; k1 = ea.kbuf[j][n + g]; k2 = ea.kbuf[j][2 * n + g]; }
+          lo[0] = FA(lo[0], FM(c, k0));
+          lo[1] = FA(lo[1], FM(c, k1));
+          lo[2] = FA(lo[2], FM(c, k2));
+        }
+        float d0 = fabsf(FA(lo[0], FM(-1.f, q[0])));
+        float d1 = fabsf(FA(lo[1], FM(-1.f, q[1])));
+        float d2 = fabsf(FA(lo[2], FM(-1.f, q[2])));
+        lmax = fmaxf(lmax, fmaxf(d0, fmaxf(d1, d2)));
+      }
+      ea.out1[g] = q[0];
+      ea.out1[n + g] = q[1];
+      ea.out1[2 * n + g] = q[2];
+    }
+  
+}
+
+// block-wide maximum of lmax into *ea.err (non-negative float atomics)
+template <int MODE>
+__device__ __forceinline__ void epi_flush_max(const EpiArgs& ea, float lmax) {
+  if ((MODE == EPI_HEUN2 || MODE == EPI_RK || MODE == EPI_TORQUE) && ea.err) {
+    for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(ea.err, lmax);
+  }
+}

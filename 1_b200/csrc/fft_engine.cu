@@ -22,6 +22,7 @@
 
 #include "fft_engine.cuh"
 #include "fft_passes.cuh"
+#include "fft_fixed_kernels.cuh"
 
 bool fft_factor(int L, LineFFT* f) {
   f->L = L;
@@ -77,6 +78,16 @@ const float2* fft_twiddles(int Lt) {
 // ---------------------------------------------------------------------
 cudaError_t launch_z_r2c(const float* src, float2* dst, const ZPass& zp, cudaStream_t st, const ZComb* cb) {
   int M = zp.f.L;
+  if (fx_ok(M)) {
+    ZComb none;
+    memset(&none, 0, sizeof(none));
+    switch (M) {
+#define C_(L) \
+  case L: return cb ? fx_launch_zr2c<L, true>(src, dst, zp, *cb, st) : fx_launch_zr2c<L, false>(src, dst, zp, none, st);
+      FX_SIZES(C_)
+#undef C_
+    }
+  }
   int lines = 1;
   while (M * lines * 2 <= (is_pow2(M) ? 4096 : 2048) && lines * 2 <= zp.nrows) lines *= 2;
   size_t smem = sizeof(float2) * (size_t)M * lines;
@@ -97,6 +108,14 @@ cudaError_t launch_z_r2c(const float* src, float2* dst, const ZPass& zp, cudaStr
 
 cudaError_t launch_z_c2r(const float2* src, float* dst, const ZPass& zp, cudaStream_t st) {
   int M = zp.f.L;
+  if (fx_ok(M)) {
+    switch (M) {
+#define C_(L) \
+  case L: return fx_launch_zc2r<L>(src, dst, zp, st);
+      FX_SIZES(C_)
+#undef C_
+    }
+  }
   int lines = 1;
   while ((M + 1) * lines * 2 <= (is_pow2(M) ? 4096 : 2048) && lines * 2 <= zp.nrows) lines *= 2;
   size_t smem = sizeof(float2) * (size_t)(M + 1) * lines;
@@ -110,6 +129,14 @@ cudaError_t launch_z_c2r(const float2* src, float* dst, const ZPass& zp, cudaStr
 
 cudaError_t launch_col(const float2* src, float2* dst, const ColPass& cp, cudaStream_t st) {
   int L = cp.f.L;
+  if (fx_ok(L)) {
+    switch (L) {
+#define C_(LL) \
+  case LL: return cp.inv ? fx_launch_col<LL, true>(src, dst, cp, st) : fx_launch_col<LL, false>(src, dst, cp, st);
+      FX_SIZES(C_)
+#undef C_
+    }
+  }
   int tk = 1;
   while (tk < 32 && L * tk * 2 <= (is_pow2(L) ? 4096 : 2048) && tk * 2 <= cp.ncols) tk *= 2;
   size_t smem = sizeof(float2) * (size_t)L * tk;

@@ -1,0 +1,465 @@
+// Fixed-size (power-of-two) pass kernels of the zero-aware padded FFT.
+// Drop-in replacements for k_col / k_z_r2c / k_z_c2r (fft_passes.cuh) and
+// for the fused k_xconv / k_yconv2d / k_zinv_epi (solver.cu) when the line
+// length is a power of two between 4 and 4096.
+#pragma once
+#include "epilogue.cuh"
+#include "kernmul.cuh"
+#include "fft_fixed.cuh"
+#include "fft_passes.cuh"
+
+// ---------------------------------------------------------------------
+// Column pass: TK adjacent columns x L, index-major tile (s[i*TK + l]).
+// Stage 0 loads from global (rows >= n_in are zero), the last stage stores
+// to global (only rows < n_out).
+// ---------------------------------------------------------------------
+template <int L, int TK, int T, bool INV>
+__global__ void __launch_bounds__(T) k_col_fx(const float2* src, float2* dst, ColPass cp) {
+  __shared__ float2 tw[L];
+  extern __shared__ float2 sm[];
+  constexpr int NST = n_stages(L);
+  load_twiddles<L, T>(tw, cp.f.tw, cp.f.tws);
+  const int c0 = blockIdx.x * TK;
+  const int64_t pbase = (int64_t)blockIdx.y * cp.plane_stride + c0;
+  const int nc = min(TK, cp.ncols - c0);
+  const int64_t sti = cp.stride_i;
+  const int n_in = cp.n_in, n_out = cp.n_out;
+  constexpr int R0 = INV ? inv_radix(L, 0) : fwd_radix(L, 0);
+  using S0 = St<L, R0, 1, TK, T, true>;
+  float2 v[S0::NB][R0];
+#pragma unroll
+  for (int i = 0; i < S0::NB; i++) {
+    if (!S0::valid(i)) continue;
+    int l, j;
+    S0::lj(i, l, j);
+#pragma unroll
+    for (int q = 0; q < R0; q++) {
+      int idx = S0::in_idx(j, q);
+      v[i][q] = (idx < n_in && l < nc) ? src[pbase + idx * sti + l] : make_float2(0.f, 0.f);
+    }
+    dft<R0>(v[i], INV);
+  }
+  if constexpr (NST == 1) {
+#pragma unroll
+    for (int i = 0; i < S0::NB; i++) {
+      if (!S0::valid(i)) continue;
+      int l, j;
+      S0::lj(i, l, j);
+#pragma unroll
+      for (int q = 0; q < R0; q++) {
+        int idx = S0::out_idx(j, q);
+        if (idx < n_out && l < nc) dst[pbase + idx * sti + l] = v[i][q];
+      }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < S0::NB; i++) {
+      if (!S0::valid(i)) continue;
+      int l, j;
+      S0::lj(i, l, j);
+#pragma unroll
+      for (int q = 0; q < R0; q++) sm[S0::out_idx(j, q) * TK + l] = v[i][q];
+    }
+    __syncthreads();
+    MidStages<L, 1, NST - 1, TK, T, true, TK, 1, INV>::run(sm, tw);
+    constexpr int RL = INV ? inv_radix(L, NST - 1) : fwd_radix(L, NST - 1);
+    constexpr int NSL = INV ? inv_span(L, NST - 1) : fwd_span(L, NST - 1);
+    using SL = St<L, RL, NSL, TK, T, true>;
+    float2 w[SL::NB][RL];
+#pragma unroll
+    for (int i = 0; i < SL::NB; i++) {
+      if (!SL::valid(i)) continue;
+      int l, j;
+      SL::lj(i, l, j);
+#pragma unroll
+      for (int q = 0; q < RL; q++) w[i][q] = sm[SL::in_idx(j, q) * TK + l];
+      SL::twiddle(w[i], j, tw, INV);
+      dft<RL>(w[i], INV);
+#pragma unroll
+      for (int q = 0; q < RL; q++) {
+        int idx = SL::out_idx(j, q);
+        if (idx < n_out && l < nc) dst[pbase + idx * sti + l] = w[i][q];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------
+// Fused convolution pass: forward transform of the three components along
+// the padded axis, multiplication by the symmetric kernel, inverse
+// transform.  3D (D2 = false): X axis, columns = flattened (ky, kz);
+// 2D (D2 = true): Y axis, columns = kz.  Tile element (c, t, i) at
+// sm[i * 3TK + c * TK + t].  The last forward stage, the kernel product and
+// the first inverse stage stay in the registers of one thread, which owns
+// the three components of its (column, butterfly).
+// ---------------------------------------------------------------------
+struct ConvArgs {
+  float2* S;
+  KernOct K;
+  int n_data;       // data rows along the transformed axis (N0 or N1)
+  int ncols;        // P1*HZ (3D) or HZ (2D)
+  int HZ;
+  int64_t stride;   // element stride along the transformed axis
+  int64_t CS;       // component stride
+  const float2* tw; // twiddles of the transformed length
+  int tws;
+};
+
+template <int L, int R, int NS, int TK, int T>
+using St3 = St<L, R, NS, TK, T, true>;  // (t, j) butterflies, components looped inside
+
+template <int L, int TK, int T, bool D2>
+__global__ void __launch_bounds__(T) k_conv_fx(ConvArgs a) {
+  __shared__ float2 tw[L];
+  extern __shared__ float2 sm[];
+  constexpr int NST = n_stages(L);
+  constexpr int NL = 3 * TK;
+  load_twiddles<L, T>(tw, a.tw, a.tws);
+  const int col0 = blockIdx.x * TK;
+  const int nc = min(TK, a.ncols - col0);
+  const int nd = a.n_data;
+  // ---- forward stage 0 from global ----
+  constexpr int R0 = fwd_radix(L, 0);
+  using S0 = St3<L, R0, 1, TK, T>;
+  // ---- registers of the last forward / first inverse stage ----
+  constexpr int RL = fwd_radix(L, NST - 1);
+  constexpr int NSL = fwd_span(L, NST - 1);
+  using SL = St3<L, RL, NSL, TK, T>;
+  float2 v[SL::NB][3][RL];
+  if constexpr (NST == 1) {
+#pragma unroll
+    for (int i = 0; i < S0::NB; i++) {
+      if (!S0::valid(i)) continue;
+      int t, j;
+      S0::lj(i, t, j);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+#pragma unroll
+        for (int q = 0; q < R0; q++) {
+          int idx = S0::in_idx(j, q);
+          v[i][c][q] = (idx < nd && t < nc) ? a.S[c * a.CS + idx * a.stride + col0 + t] : make_float2(0.f, 0.f);
+        }
+        dft<R0>(v[i][c], false);
+      }
+    }
+  } else {
+    float2 u[S0::NB][3][R0];
+#pragma unroll
+    for (int i = 0; i < S0::NB; i++) {
+      if (!S0::valid(i)) continue;
+      int t, j;
+      S0::lj(i, t, j);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+#pragma unroll
+        for (int q = 0; q < R0; q++) {
+          int idx = S0::in_idx(j, q);
+          u[i][c][q] = (idx < nd && t < nc) ? a.S[c * a.CS + idx * a.stride + col0 + t] : make_float2(0.f, 0.f);
+        }
+        dft<R0>(u[i][c], false);
+#pragma unroll
+        for (int q = 0; q < R0; q++) sm[S0::out_idx(j, q) * NL + c * TK + t] = u[i][c][q];
+      }
+    }
+    __syncthreads();
+    MidStages<L, 1, NST - 1, NL, T, true, NL, 1, false>::run(sm, tw);
+#pragma unroll
+    for (int i = 0; i < SL::NB; i++) {
+      if (!SL::valid(i)) continue;
+      int t, j;
+      SL::lj(i, t, j);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+#pragma unroll
+        for (int q = 0; q < RL; q++) v[i][c][q] = sm[SL::in_idx(j, q) * NL + c * TK + t];
+        SL::twiddle(v[i][c], j, tw, false);
+        dft<RL>(v[i][c], false);
+      }
+    }
+  }
+  // ---- kernel multiplication, H = K M per bin ----
+#pragma unroll
+  for (int i = 0; i < SL::NB; i++) {
+    if (!SL::valid(i)) continue;
+    int t, j;
+    SL::lj(i, t, j);
+    if (t >= nc) continue;
+    int col = col0 + t;
+    int kyc, kzc;
+    if (D2) { kyc = 0; kzc = col; }
+    else { kyc = col / a.HZ; kzc = col - kyc * a.HZ; }
+#pragma unroll
+    for (int q = 0; q < RL; q++) {
+      int k = SL::out_idx(j, q);
+      float Kxx, Kyy, Kzz, Kyz, Kxz, Kxy;
+      if (D2) {
+        kern_at(a.K, 0, k, kzc, Kxx, Kyy, Kzz, Kyz, Kxz, Kxy);
+        kmul4(v[i][0][q], v[i][1][q], v[i][2][q], Kxx, Kyy, Kzz, Kyz);
+      } else {
+        kern_at(a.K, k, kyc, kzc, Kxx, Kyy, Kzz, Kyz, Kxz, Kxy);
+        kmul6(v[i][0][q], v[i][1][q], v[i][2][q], Kxx, Kyy, Kzz, Kyz, Kxz, Kxy);
+      }
+    }
+  }
+  // ---- inverse: first stage in registers (same grouping) ----
+  if constexpr (NST == 1) {
+#pragma unroll
+    for (int i = 0; i < SL::NB; i++) {
+      if (!SL::valid(i)) continue;
+      int t, j;
+      SL::lj(i, t, j);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        dft<RL>(v[i][c], true);
+#pragma unroll
+        for (int q = 0; q < RL; q++) {
+          int idx = SL::out_idx(j, q);
+          if (idx < nd && t < nc) a.S[c * a.CS + idx * a.stride + col0 + t] = v[i][c][q];
+        }
+      }
+    }
+  } else {
+    using I0 = St3<L, inv_radix(L, 0), 1, TK, T>;  // same radix and butterflies as SL
+    static_assert(inv_radix(L, 0) == RL && I0::M == NSL, "grouping mismatch");
+    __syncthreads();  // the last forward stage read the tile
+#pragma unroll
+    for (int i = 0; i < SL::NB; i++) {
+      if (!SL::valid(i)) continue;
+      int t, j;
+      SL::lj(i, t, j);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        dft<RL>(v[i][c], true);
+#pragma unroll
+        for (int q = 0; q < RL; q++) sm[I0::out_idx(j, q) * NL + c * TK + t] = v[i][c][q];
+      }
+    }
+    __syncthreads();
+    MidStages<L, 1, NST - 1, NL, T, true, NL, 1, true>::run(sm, tw);
+    constexpr int RI = inv_radix(L, NST - 1);
+    constexpr int NSI = inv_span(L, NST - 1);
+    using SI = St3<L, RI, NSI, TK, T>;
+#pragma unroll
+    for (int i = 0; i < SI::NB; i++) {
+      if (!SI::valid(i)) continue;
+      int t, j;
+      SI::lj(i, t, j);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        float2 w[RI];
+#pragma unroll
+        for (int q = 0; q < RI; q++) w[q] = sm[SI::in_idx(j, q) * NL + c * TK + t];
+        SI::twiddle(w, j, tw, true);
+        dft<RI>(w, true);
+#pragma unroll
+        for (int q = 0; q < RI; q++) {
+          int idx = SI::out_idx(j, q);
+          if (idx < nd && t < nc) a.S[c * a.CS + idx * a.stride + col0 + t] = w[q];
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------
+// Z rows.  Tile index-major with an odd row pitch: element n of line l at
+// sm[n * SIP + l]; global accesses walk the row (coalesced), stages walk
+// the lines (conflict-free).
+// ---------------------------------------------------------------------
+__host__ __device__ constexpr int odd_pitch(int lines) { return (lines % 2) ? lines : lines + 1; }
+
+template <int M, int RT, int T, bool COMB>
+__global__ void __launch_bounds__(T) k_zr2c_fx(const float* __restrict__ src, float2* __restrict__ dst, ZPass z,
+                                               ZComb cb) {
+  __shared__ float2 tw[M];
+  extern __shared__ float2 sm[];
+  constexpr int SIP = odd_pitch(RT);
+  load_twiddles<M, T>(tw, z.f.tw, z.f.tws);
+  const int r0 = blockIdx.x * RT;
+  const int nl = min(RT, z.nrows - r0);
+  const float dt = COMB ? *cb.dt : 0.f;
+  for (int e = threadIdx.x; e < RT * M; e += T) {
+    int l = e / M, n = e - l * M;
+    float a = 0.f, b = 0.f;
+    if (l < nl) {
+      int64_t roff, soff;
+      zrow_offsets(z, r0 + l, &roff, &soff);
+      int i0 = 2 * n, i1 = 2 * n + 1;
+      if (COMB) {
+        if (i0 < z.n_real) { a = zcomb_value(cb, dt, roff + i0); cb.out[roff + i0] = a; }
+        if (i1 < z.n_real) { b = zcomb_value(cb, dt, roff + i1); cb.out[roff + i1] = b; }
+      } else {
+        const float* row = src + roff;
+        if (i0 < z.n_real) a = row[i0];
+        if (i1 < z.n_real) b = row[i1];
+      }
+    }
+    sm[n * SIP + l] = make_float2(a, b);
+  }
+  __syncthreads();
+  tile_fft_fixed<M, RT, T, true, SIP, 1, false>(sm, tw);
+  for (int e = threadIdx.x; e < nl * (M + 1); e += T) {
+    int l = e / (M + 1), k = e - l * (M + 1);
+    int64_t roff, soff;
+    zrow_offsets(z, r0 + l, &roff, &soff);
+    float2 Zk = sm[(k == M ? 0 : k) * SIP + l];
+    float2 Zm = sm[(k == 0 ? 0 : M - k) * SIP + l];
+    float2 E = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+    float2 O = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+    float2 w = __ldg(&z.twP[k]);
+    float2 wo = cmul_f(w, O);
+    dst[soff + k] = make_float2(E.x + wo.x, E.y + wo.y);
+  }
+}
+
+// Z'_k = (X_k + conj X_{M-k}) + i (X_k - conj X_{M-k}) w^{-k}; X_0, X_M real
+__device__ __forceinline__ float2 c2r_pre(float2 Xk, float2 Xm, int k, int M, const float2* __restrict__ twP) {
+  if (k == 0) { Xk.y = 0.f; Xm.y = 0.f; }
+  float2 A = make_float2(Xk.x + Xm.x, Xk.y - Xm.y);
+  float2 B = make_float2(Xk.x - Xm.x, Xk.y + Xm.y);
+  float2 w = __ldg(&twP[k]);
+  float2 C = cmulc_f(B, w);
+  return make_float2(A.x - C.y, A.y + C.x);
+}
+
+template <int M, int RT, int T>
+__global__ void __launch_bounds__(T) k_zc2r_fx(const float2* __restrict__ src, float* __restrict__ dst, ZPass z) {
+  __shared__ float2 tw[M];
+  extern __shared__ float2 sm[];
+  constexpr int SIP = odd_pitch(RT);
+  load_twiddles<M, T>(tw, z.f.tw, z.f.tws);
+  const int r0 = blockIdx.x * RT;
+  const int nl = min(RT, z.nrows - r0);
+  for (int e = threadIdx.x; e < RT * M; e += T) {
+    int l = e / M, k = e - l * M;
+    float2 v = make_float2(0.f, 0.f);
+    if (l < nl) {
+      int64_t roff, soff;
+      zrow_offsets(z, r0 + l, &roff, &soff);
+      v = c2r_pre(src[soff + k], src[soff + M - k], k, M, z.twP);
+    }
+    sm[k * SIP + l] = v;
+  }
+  __syncthreads();
+  tile_fft_fixed<M, RT, T, true, SIP, 1, true>(sm, tw);
+  for (int e = threadIdx.x; e < nl * M; e += T) {
+    int l = e / M, n = e - l * M;
+    int i0 = 2 * n;
+    if (i0 >= z.n_real) continue;
+    int64_t roff, soff;
+    zrow_offsets(z, r0 + l, &roff, &soff);
+    float2 v = sm[n * SIP + l];
+    dst[roff + i0] = v.x;
+    if (i0 + 1 < z.n_real) dst[roff + i0 + 1] = v.y;
+  }
+}
+
+// Inverse Z of the three components of RT spatial rows + the solver epilogue.
+template <int M, int RT, int T, int MODE>
+__global__ void __launch_bounds__(T) k_zinv_fx(const float2* __restrict__ S, const float2* __restrict__ twz,
+                                               const float2* __restrict__ twP, int P1, int HZ, int64_t CS, int nrows,
+                                               EpiArgs ea) {
+  __shared__ float2 tw[M];
+  extern __shared__ float2 sm[];
+  constexpr int NL = 3 * RT;
+  constexpr int SIP = odd_pitch(NL);
+  load_twiddles<M, T>(tw, twz, 2);
+  const int r0 = blockIdx.x * RT;
+  const int nr = min(RT, nrows - r0);
+  const int N1 = ea.N1, N2 = ea.N2;
+  for (int e = threadIdx.x; e < NL * M; e += T) {
+    int l = e / M, k = e - l * M;
+    int r = l / 3, c = l - 3 * r;
+    float2 v = make_float2(0.f, 0.f);
+    if (r < nr) {
+      int gr = r0 + r;
+      int x = gr / N1, y = gr - x * N1;
+      const float2* row = S + c * CS + ((int64_t)x * P1 + y) * HZ;
+      v = c2r_pre(row[k], row[M - k], k, M, twP);
+    }
+    sm[k * SIP + l] = v;
+  }
+  __syncthreads();
+  tile_fft_fixed<M, NL, T, true, SIP, 1, true>(sm, tw);
+  float lmax = 0.f;
+  for (int e = threadIdx.x; e < nr * N2; e += T) {
+    int r = e / N2, zz = e - r * N2;
+    int64_t g = (int64_t)(r0 + r) * N2 + zz;
+    const float2* base = sm + (zz >> 1) * SIP + 3 * r;
+    float hx = (zz & 1) ? base[0].y : base[0].x;
+    float hy = (zz & 1) ? base[1].y : base[1].x;
+    float hz = (zz & 1) ? base[2].y : base[2].x;
+    epi_cell<MODE>(ea, g, hx, hy, hz, lmax);
+  }
+  epi_flush_max<MODE>(ea, lmax);
+}
+
+// ---------------------------------------------------------------------
+// Launch-shape tables.  Every tile holds about 4096 complex values and
+// every thread about 16 (512 threads for the longest lines).
+// ---------------------------------------------------------------------
+#define FX_SIZES(X) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
+static inline bool fx_ok(int L) { return L >= 8 && L <= 4096 && (L & (L - 1)) == 0; }
+
+__host__ __device__ constexpr int fx_col_tk(int L) { return L >= 4096 ? 1 : (4096 / L > 32 ? 32 : 4096 / L); }
+__host__ __device__ constexpr int fx_threads(int elems) {
+  return elems / 16 < 64 ? 64 : (elems / 16 > 512 ? 512 : ((elems / 16 + 31) / 32) * 32);
+}
+
+template <int L, bool INV>
+cudaError_t fx_launch_col(const float2* src, float2* dst, const ColPass& cp, cudaStream_t st) {
+  constexpr int TK = fx_col_tk(L);
+  constexpr int T = fx_threads(TK * L);
+  size_t smem = sizeof(float2) * (size_t)TK * L;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_col_fx<L, TK, T, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  dim3 grid(div_up(cp.ncols, TK), cp.nplanes);
+  k_col_fx<L, TK, T, INV><<<grid, T, smem, st>>>(src, dst, cp);
+  return cudaGetLastError();
+}
+
+template <int L, bool D2>
+cudaError_t fx_launch_conv(const ConvArgs& a, cudaStream_t st) {
+  constexpr int TK = L >= 2048 ? 1 : (1365 / L > 32 ? 32 : (1365 / L < 1 ? 1 : 1365 / L)) ;
+  constexpr int TKP = TK >= 16 ? 16 : (TK >= 8 ? 8 : (TK >= 4 ? 4 : (TK >= 2 ? 2 : 1)));
+  // one thread per (column, radix-8 butterfly): it owns the three components
+  constexpr int T = (TKP * L / 8) < 64 ? 64 : ((TKP * L / 8) > 512 ? 512 : (TKP * L / 8));
+  size_t smem = sizeof(float2) * (size_t)3 * TKP * L;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_conv_fx<L, TKP, T, D2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_conv_fx<L, TKP, T, D2><<<div_up(a.ncols, TKP), T, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+__host__ __device__ constexpr int fx_rows(int M, int lines_per_row) {
+  return (4096 / (M * lines_per_row)) < 1 ? 1 : (4096 / (M * lines_per_row) > 32 ? 32 : 4096 / (M * lines_per_row));
+}
+
+template <int M, bool COMB>
+cudaError_t fx_launch_zr2c(const float* src, float2* dst, const ZPass& z, const ZComb& cb, cudaStream_t st) {
+  constexpr int RT = fx_rows(M, 1);
+  constexpr int T = fx_threads(RT * M);
+  size_t smem = sizeof(float2) * (size_t)odd_pitch(RT) * M;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_zr2c_fx<M, RT, T, COMB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_zr2c_fx<M, RT, T, COMB><<<div_up(z.nrows, RT), T, smem, st>>>(src, dst, z, cb);
+  return cudaGetLastError();
+}
+
+template <int M>
+cudaError_t fx_launch_zc2r(const float2* src, float* dst, const ZPass& z, cudaStream_t st) {
+  constexpr int RT = fx_rows(M, 1);
+  constexpr int T = fx_threads(RT * M);
+  size_t smem = sizeof(float2) * (size_t)odd_pitch(RT) * M;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_zc2r_fx<M, RT, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_zc2r_fx<M, RT, T><<<div_up(z.nrows, RT), T, smem, st>>>(src, dst, z);
+  return cudaGetLastError();
+}
+
+template <int M, int MODE>
+cudaError_t fx_launch_zinv(const float2* S, const float2* twz, const float2* twP, int P1, int HZ, int64_t CS, int nrows,
+                           const EpiArgs& ea, cudaStream_t st) {
+  constexpr int RT = fx_rows(M, 3);
+  constexpr int T = fx_threads(3 * RT * M);
+  size_t smem = sizeof(float2) * (size_t)odd_pitch(3 * RT) * M;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_zinv_fx<M, RT, T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_zinv_fx<M, RT, T, MODE><<<div_up(nrows, RT), T, smem, st>>>(S, twz, twP, P1, HZ, CS, nrows, ea);
+  return cudaGetLastError();
+}

@@ -28,6 +28,9 @@
 #include "demag_gpu.cuh"
 #include "fft_passes.cuh"
 #include "llg_ops.cuh"
+#include "epilogue.cuh"
+#include "kernmul.cuh"
+#include "fft_fixed_kernels.cuh"
 #include "../../include/mmx.h"
 
 static thread_local std::string g_err = "";
@@ -46,14 +49,8 @@ int mmx_sm_count() {
 }
 
 // ---------------------------------------------------------------------
-// Kernel octant
+// Kernel octant extraction (the octant layout is in kernmul.cuh)
 // ---------------------------------------------------------------------
-struct KernOct {
-  const float* kh;  // [6][O0][O1][HZ]
-  int O0, O1, HZ, P0, P1;
-  int64_t cs;       // component stride
-};
-
 __global__ void k_extract_octant(const float2* __restrict__ spec, float* __restrict__ kh, int O0, int O1, int P1,
                                  int HZ, float norm) {
   int64_t n = (int64_t)O0 * O1 * HZ;
@@ -63,52 +60,6 @@ __global__ void k_extract_octant(const float2* __restrict__ spec, float* __restr
     int kx = (int)(e / ((int64_t)HZ * O1));
     kh[e] = __fmul_rn(spec[((int64_t)kx * P1 + ky) * HZ + kz].x, norm);
   }
-}
-
-__device__ __forceinline__ void kern_at(const KernOct& K, int kx, int ky, int kz, float& Kxx, float& Kyy,
-                                        float& Kzz, float& Kyz, float& Kxz, float& Kxy) {
-  int fx = kx <= K.P0 / 2 ? kx : K.P0 - kx;
-  int fy = ky <= K.P1 / 2 ? ky : K.P1 - ky;
-  bool nx = kx > K.P0 / 2, ny = ky > K.P1 / 2;
-  int64_t o = ((int64_t)fx * K.O1 + fy) * K.HZ + kz;
-  Kxx = __ldg(K.kh + o);
-  Kyy = __ldg(K.kh + K.cs + o);
-  Kzz = __ldg(K.kh + 2 * K.cs + o);
-  Kyz = __ldg(K.kh + 3 * K.cs + o);
-  Kxz = __ldg(K.kh + 4 * K.cs + o);
-  Kxy = __ldg(K.kh + 5 * K.cs + o);
-  if (ny) Kyz = -Kyz;
-  if (nx) Kxz = -Kxz;
-  if (nx != ny) Kxy = -Kxy;
-}
-
-// H = K M per bin in the order of gpu_kernelmul6 (gpu_kernmul.cu:51-58)
-__device__ __forceinline__ void kmul6(float2& mx, float2& my, float2& mz, float Kxx, float Kyy, float Kzz, float Kyz,
-                                      float Kxz, float Kxy) {
-  float2 hx, hy, hz;
-  hx.x = FA(FA(FM(mx.x, Kxx), FM(my.x, Kxy)), FM(mz.x, Kxz));
-  hx.y = FA(FA(FM(mx.y, Kxx), FM(my.y, Kxy)), FM(mz.y, Kxz));
-  hy.x = FA(FA(FM(mx.x, Kxy), FM(my.x, Kyy)), FM(mz.x, Kyz));
-  hy.y = FA(FA(FM(mx.y, Kxy), FM(my.y, Kyy)), FM(mz.y, Kyz));
-  hz.x = FA(FA(FM(mx.x, Kxz), FM(my.x, Kyz)), FM(mz.x, Kzz));
-  hz.y = FA(FA(FM(mx.y, Kxz), FM(my.y, Kyz)), FM(mz.y, Kzz));
-  mx = hx;
-  my = hy;
-  mz = hz;
-}
-// 2D: Kxy = Kxz = 0 (gpu_kernmul.cu:114-119)
-__device__ __forceinline__ void kmul4(float2& mx, float2& my, float2& mz, float Kxx, float Kyy, float Kzz,
-                                      float Kyz) {
-  float2 hx, hy, hz;
-  hx.x = FM(mx.x, Kxx);
-  hx.y = FM(mx.y, Kxx);
-  hy.x = FA(FM(my.x, Kyy), FM(mz.x, Kyz));
-  hy.y = FA(FM(my.y, Kyy), FM(mz.y, Kyz));
-  hz.x = FA(FM(my.x, Kyz), FM(mz.x, Kzz));
-  hz.y = FA(FM(my.y, Kyz), FM(mz.y, Kzz));
-  mx = hx;
-  my = hy;
-  mz = hz;
 }
 
 // ---------------------------------------------------------------------
@@ -200,34 +151,6 @@ __global__ void FFT_BOUNDS(THREADS) k_yconv2d(float2* __restrict__ S, LineFFT fy
 // Zi + epilogue: inverse Z (C2R) of the three components of R rows in
 // shared memory, then the per-cell solver update.
 // ---------------------------------------------------------------------
-enum { EPI_FIELD = 0, EPI_HEUN1 = 1, EPI_HEUN2 = 2, EPI_TORQUE = 3, EPI_RK = 4 };
-
-#define RK_MAXS 7
-struct RKCoef {
-  float a[RK_MAXS];   // row a[i+1][0..i] (next stage input), or b for the final stage
-  float b2[RK_MAXS];  // lower-order weights (final stage, adaptive)
-  int nk;             // number of k's combined
-  int final_stage;    // 1: produce m_high / m_low / error
-  int adaptive;
-};
-
-struct EpiArgs {
-  int N1, N2;
-  int64_t n;            // cells per component
-  LocalField lf;
-  float alpha, dtg;
-  const float* m_in;    // magnetisation at which the field was evaluated
-  float* out0;
-  float* out1;
-  const float* aux0;
-  const float* aux1;
-  float* err;           // device scalar (maxabs target), may be null
-  const float* dt_dev;  // RK: device dt
-  float* kbuf[RK_MAXS]; // RK: stage torques
-  int stage;            // RK: index of this stage's k
-  RKCoef rk;
-};
-
 template <int THREADS, int EPT, bool POW2, int MODE>
 __global__ void FFT_BOUNDS(THREADS) k_zinv_epi(const float2* __restrict__ S, LineFFT fz,
                                                   const float2* __restrict__ twP, int N0, int P1, int HZ, int64_t CS,
@@ -290,100 +213,9 @@ __global__ void FFT_BOUNDS(THREADS) k_zinv_epi(const float2* __restrict__ S, Lin
     float hx = (z & 1) ? base[0].y : base[0].x;
     float hy = (z & 1) ? base[ld].y : base[ld].x;
     float hz = (z & 1) ? base[2 * ld].y : base[2 * ld].x;
-    const int64_t n = ea.n;
-    float mx = ea.m_in[g], my = ea.m_in[n + g], mz = ea.m_in[2 * n + g];
-    llg_local(ea.lf, mx, my, mz, hx, hy, hz);
-    if (MODE == EPI_FIELD) {
-      ea.out0[g] = hx;
-      ea.out0[n + g] = hy;
-      ea.out0[2 * n + g] = hz;
-      continue;
-    }
-    llg_delta_m(mx, my, mz, hx, hy, hz, ea.alpha, ea.dtg);
-    if (MODE == EPI_TORQUE) {
-      ea.out0[g] = hx;
-      ea.out0[n + g] = hy;
-      ea.out0[2 * n + g] = hz;
-      if (ea.err) lmax = fmaxf(lmax, fmaxf(fabsf(hx), fmaxf(fabsf(hy), fabsf(hz))));
-    } else if (MODE == EPI_HEUN1) {
-      // t0 = torque*dt; m1est = normalize(m + t0)   (adaptive_heun.go:141-146)
-      ea.out0[g] = hx;
-      ea.out0[n + g] = hy;
-      ea.out0[2 * n + g] = hz;
-      float ex = FA(mx, hx), ey = FA(my, hy), ez = FA(mz, hz);
-      llg_normalize(ex, ey, ez);
-      ea.out1[g] = ex;
-      ea.out1[n + g] = ey;
-      ea.out1[2 * n + g] = ez;
-    } else if (MODE == EPI_HEUN2) {
-      // t = 0.5 t1 + 0.5 t0; m = normalize(m + t)   (adaptive_heun.go:148-154)
-      float tx = FA(FM(0.5f, hx), FM(0.5f, ea.aux0[g]));
-      float ty = FA(FM(0.5f, hy), FM(0.5f, ea.aux0[n + g]));
-      float tz = FA(FM(0.5f, hz), FM(0.5f, ea.aux0[2 * n + g]));
-      float nx = FA(ea.aux1[g], tx), ny = FA(ea.aux1[n + g], ty), nz = FA(ea.aux1[2 * n + g], tz);
-      llg_normalize(nx, ny, nz);
-      ea.out0[g] = nx;
-      ea.out0[n + g] = ny;
-      ea.out0[2 * n + g] = nz;
-      if (ea.err) {
-        // error = maxabs(m1est - m)   (adaptive_heun.go:158-160)
-        float d0 = fabsf(FA(mx, FM(-1.f, nx)));
-        float d1 = fabsf(FA(my, FM(-1.f, ny)));
-        float d2 = fabsf(FA(mz, FM(-1.f, nz)));
-        lmax = fmaxf(lmax, fmaxf(d0, fmaxf(d1, d2)));
-      }
-    } else if (MODE == EPI_RK) {
-      float kx = hx, ky = hy, kz = hz;
-      float* kd = ea.out0;
-      kd[g] = kx;
-      kd[n + g] = ky;
-      kd[2 * n + g] = kz;
-      const float dt = *ea.dt_dev;
-      const float* m0 = ea.aux0;  // step start magnetisation
-      float q[3] = {m0[g], m0[n + g], m0[2 * n + g]};
-      // next stage input (or m_high): m0 + sum_j (dt a_j) k_j, j in order
-#pragma unroll
-      for (int j = 0; j < RK_MAXS; j++) {
-        if (j >= ea.rk.nk) break;
-        float a = ea.rk.a[j];
-        if (a == 0.f) continue;
-        float c = FM(dt, a);
-        float k0, k1, k2;
-        if (j == ea.stage) { k0 = kx; k1 = ky; k2 = kz; }
-        else { k0 = ea.kbuf[j][g]; k1 = ea.kbuf[j][n + g]; k2 = ea.kbuf[j][2 * n + g]; }
-        q[0] = FA(q[0], FM(c, k0));
-        q[1] = FA(q[1], FM(c, k1));
-        q[2] = FA(q[2], FM(c, k2));
-      }
-      if (ea.rk.final_stage && ea.rk.adaptive) {
-        float lo[3] = {m0[g], m0[n + g], m0[2 * n + g]};
-#pragma unroll
-        for (int j = 0; j < RK_MAXS; j++) {
-          if (j >= ea.rk.nk) break;
-          float b = ea.rk.b2[j];
-          if (b == 0.f) continue;
-          float c = FM(b, dt);
-          float k0, k1, k2;
-          if (j == ea.stage) { k0 = kx; k1 = ky; k2 = kz; }
-          else { k0 = ea.kbuf[j][g]; k1 = ea.kbuf[j][n + g]; k2 = ea.kbuf[j][2 * n + g]; }
-          lo[0] = FA(lo[0], FM(c, k0));
-          lo[1] = FA(lo[1], FM(c, k1));
-          lo[2] = FA(lo[2], FM(c, k2));
-        }
-        float d0 = fabsf(FA(lo[0], FM(-1.f, q[0])));
-        float d1 = fabsf(FA(lo[1], FM(-1.f, q[1])));
-        float d2 = fabsf(FA(lo[2], FM(-1.f, q[2])));
-        lmax = fmaxf(lmax, fmaxf(d0, fmaxf(d1, d2)));
-      }
-      ea.out1[g] = q[0];
-      ea.out1[n + g] = q[1];
-      ea.out1[2 * n + g] = q[2];
-    }
+    epi_cell<MODE>(ea, g, hx, hy, hz, lmax);
   }
-  if ((MODE == EPI_HEUN2 || MODE == EPI_RK || MODE == EPI_TORQUE) && ea.err) {
-    for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(ea.err, lmax);
-  }
+  epi_flush_max<MODE>(ea, lmax);
 }
 
 // ---------------------------------------------------------------------
@@ -564,6 +396,25 @@ static void flush_timers(mmx_solver* s) {
 
 static cudaError_t launch_xconv(mmx_solver* s, cudaStream_t st) {
   int P0 = s->P[0];
+  if (fx_ok(P0)) {
+    ConvArgs a;
+    a.S = s->S;
+    a.K = s->K;
+    a.n_data = s->N[0];
+    a.ncols = s->P[1] * s->HZ;
+    a.HZ = s->HZ;
+    a.stride = (int64_t)s->P[1] * s->HZ;
+    a.CS = s->CS;
+    a.tw = s->bp.fx.tw;
+    a.tws = s->bp.fx.tws;
+    ScopedPass sp(s, "xconv", st);
+    switch (P0) {
+#define C_(L) \
+  case L: return fx_launch_conv<L, false>(a, st);
+      FX_SIZES(C_)
+#undef C_
+    }
+  }
   int tk = 1;
   while (tk < 32 && P0 * 3 * tk * 2 <= (is_pow2(P0) ? 4096 : 2048)) tk *= 2;
   size_t smem = sizeof(float2) * (size_t)P0 * 3 * tk;
@@ -578,6 +429,25 @@ static cudaError_t launch_xconv(mmx_solver* s, cudaStream_t st) {
 
 static cudaError_t launch_yconv2d(mmx_solver* s, cudaStream_t st) {
   int P1 = s->P[1];
+  if (fx_ok(P1)) {
+    ConvArgs a;
+    a.S = s->S;
+    a.K = s->K;
+    a.n_data = s->N[1];
+    a.ncols = s->HZ;
+    a.HZ = s->HZ;
+    a.stride = s->HZ;
+    a.CS = s->CS;
+    a.tw = s->bp.fy.tw;
+    a.tws = s->bp.fy.tws;
+    ScopedPass sp(s, "yconv2d", st);
+    switch (P1) {
+#define C_(L) \
+  case L: return fx_launch_conv<L, true>(a, st);
+      FX_SIZES(C_)
+#undef C_
+    }
+  }
   int tk = 1;
   while (tk < 32 && P1 * 3 * tk * 2 <= (is_pow2(P1) ? 4096 : 2048) && tk * 2 <= s->HZ) tk *= 2;
   size_t smem = sizeof(float2) * (size_t)P1 * 3 * tk;
@@ -593,6 +463,15 @@ template <int MODE>
 static cudaError_t launch_zinv(mmx_solver* s, const EpiArgs& ea, cudaStream_t st) {
   int M = s->P[2] / 2;
   int nrows = s->N[0] * s->N[1];
+  if (fx_ok(M)) {
+    ScopedPass sp(s, "zinv_epi", st);
+    switch (M) {
+#define C_(L) \
+  case L: return fx_launch_zinv<L, MODE>(s->S, s->bp.twz, s->bp.twz, s->P[1], s->HZ, s->CS, nrows, ea, st);
+      FX_SIZES(C_)
+#undef C_
+    }
+  }
   int rows = 1;
   while (3 * (rows * 2) * (M + 1) <= (is_pow2(M) ? 4096 : 2048) && rows * 2 <= nrows) rows *= 2;
   size_t smem = sizeof(float2) * (size_t)3 * rows * (M + 1);

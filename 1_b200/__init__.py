@@ -191,6 +191,13 @@ MMX = {
     "mmx_solver_pass_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                              ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
                                              ctypes.POINTER(ctypes.c_int)]),
+    "mmx_batch_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "mmx_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "mmx_batch_instance": (ctypes.c_void_p, [ctypes.c_void_p, ctypes.c_int]),
+    "mmx_batch_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong),
+                                      ctypes.POINTER(ctypes.c_int)]),
+    "mmx_batch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "mmx_batch_use_graph": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "mmx_reduce_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                          ctypes.c_void_p]),
     "mmx_face_kernel6": (ctypes.c_int, [c_int_p, c_int_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int,
@@ -383,6 +390,79 @@ class Solver:
         n = ctypes.c_int()
         _check(lib().mmx_solver_pass_times(self.h, 32, names, ms, la, ctypes.byref(n)))
         return {names[i].value.decode(): (ms[i], la[i]) for i in range(n.value)}
+
+
+class _InstanceView(Solver):
+    """A solver owned by a batch (not destroyed on its own)."""
+
+    def __init__(self, handle, params):
+        self.params = params
+        self.h = ctypes.c_void_p(handle)
+        self.N = (params.size[0], params.size[1], params.size[2])
+        self.n = self.N[0] * self.N[1] * self.N[2]
+
+    def close(self):
+        self.h = ctypes.c_void_p()
+
+
+class Batch:
+    """Many independent instances advanced together (mmx_batch_*)."""
+
+    def __init__(self, params_list):
+        arr = (MmxParams * len(params_list))(*params_list)
+        self.h = ctypes.c_void_p()
+        _check(lib().mmx_batch_create(arr, len(params_list), ctypes.byref(self.h)))
+        self.params = list(params_list)
+        self.instances = [_InstanceView(lib().mmx_batch_instance(self.h, i), p) for i, p in enumerate(params_list)]
+
+    def close(self):
+        if self.h:
+            for v in self.instances:
+                v.close()
+            lib().mmx_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def size(self):
+        c, cells, la = ctypes.c_int(), ctypes.c_longlong(), ctypes.c_int()
+        _check(lib().mmx_batch_size(self.h, ctypes.byref(c), ctypes.byref(cells), ctypes.byref(la)))
+        return dict(count=c.value, cells=cells.value, launches_per_step=la.value)
+
+    def step(self, n=1, stream=None):
+        _check(lib().mmx_batch_step(self.h, n, stream))
+
+    def use_graph(self, on=True):
+        _check(lib().mmx_batch_use_graph(self.h, 1 if on else 0))
+
+
+def batch_config(count, seed=4, cell=3e-9, solver="rk4", dt=5e-15):
+    """The batch configuration: count instances with Nx, Ny drawn from
+    {32,48,64,96,128,192,256}, Nz from {1,2,4}, Ms ~ U[4e5,1.4e6] A/m,
+    A ~ U[5e-12,2e-11] J/m, alpha ~ U[0.01,0.5], a uniform field of random
+    direction and |B| ~ U[0,100] mT, cubic cells of 3 nm; returns the user
+    level descriptions (per-instance draw order: Nx, Ny, Nz, Ms, A, alpha,
+    field direction (3 normals), |B|)."""
+    rng = np.random.default_rng(seed)
+    sizes = [32, 48, 64, 96, 128, 192, 256]
+    out = []
+    for _ in range(count):
+        nx = int(rng.choice(sizes))
+        ny = int(rng.choice(sizes))
+        nz = int(rng.choice([1, 2, 4]))
+        ms = float(rng.uniform(4e5, 1.4e6))
+        a = float(rng.uniform(5e-12, 2e-11))
+        alpha = float(rng.uniform(0.01, 0.5))
+        d = rng.standard_normal(3)
+        d = d / np.linalg.norm(d)
+        bmag = float(rng.uniform(0.0, 0.1))
+        out.append(dict(grid=(nx, ny, nz), cell=(cell, cell, cell), msat=ms, aexch=a, alpha=alpha,
+                        bext=tuple(float(x) for x in bmag * d), solver=solver, dt=dt))
+    return out
 
 
 def face_kernel6_device(P, periodic, cellsize, exch6=True, accuracy=8, out_ptr=None, stream=None):

@@ -1,4 +1,4 @@
-// Compile-time power-of-two line FFTs for the hot passes.
+// Compile-time line FFTs for the hot passes.
 //
 // Same Stockham (self-sorting, decimation in time) formulation as
 // fft_engine.cuh, but with the line length L, the radix of every stage, the
@@ -9,11 +9,11 @@
 // store straight to global memory (pruned outputs are not stored), so a
 // transform of R^s points makes s-1 round trips through shared memory.
 //
-// Radix plan: L = 8^a * r, r in {1, 2, 4}; the forward transform applies
-// the radix-8 stages first and r last, the inverse applies them in reverse
-// order, so that the last forward stage and the first inverse stage group
-// the same elements in the same thread (the kernel multiplication between
-// them stays in registers).
+// Radix plan: radix-8 stages first, then 4 or 2, then 3, 5, 7 (a line
+// length is any product of these); the inverse applies the stages in
+// reverse order, so that the last forward stage and the first inverse stage
+// group the same elements in the same thread (the kernel multiplication
+// between them stays in registers).
 #pragma once
 #include "fft_engine.cuh"
 
@@ -27,13 +27,15 @@ __device__ __forceinline__ float2 cmulc_f(float2 a, float2 b) {  // a * conj(b)
 }
 
 __host__ __device__ constexpr int ilog2c(int x) { return x <= 1 ? 0 : 1 + ilog2c(x >> 1); }
-__host__ __device__ constexpr int rem_radix(int L) {  // r of L = 8^a * r
-  return (ilog2c(L) % 3) == 0 ? 1 : (ilog2c(L) % 3) == 1 ? 2 : 4;
+// Radix plan of a line length L = 2^a 3^b 5^c 7^d: radix 8 while 8 divides
+// the rest, then 4 or 2, then the odd radices.
+__host__ __device__ constexpr int first_radix(int L) {
+  return L % 8 == 0 ? 8 : L % 4 == 0 ? 4 : L % 2 == 0 ? 2 : L % 3 == 0 ? 3 : L % 5 == 0 ? 5 : 7;
 }
-__host__ __device__ constexpr int n_stages(int L) { return ilog2c(L) / 3 + (rem_radix(L) > 1 ? 1 : 0); }
+__host__ __device__ constexpr int n_stages(int L) { return L <= 1 ? 0 : 1 + n_stages(L / first_radix(L)); }
 // radix of forward stage st
 __host__ __device__ constexpr int fwd_radix(int L, int st) {
-  return (st < ilog2c(L) / 3) ? 8 : rem_radix(L);
+  return st == 0 ? first_radix(L) : fwd_radix(L / first_radix(L), st - 1);
 }
 // radix of inverse stage st (reverse order)
 __host__ __device__ constexpr int inv_radix(int L, int st) { return fwd_radix(L, n_stages(L) - 1 - st); }
@@ -74,7 +76,7 @@ struct St {
     int k = j % NS;
 #pragma unroll
     for (int q = 1; q < R; q++) {
-      float2 w = tw[(q * k * TSTEP) & (L - 1)];
+      float2 w = tw[q * k * TSTEP];
       v[q] = inv ? cmulc_f(v[q], w) : cmul_f(v[q], w);
     }
   }

@@ -1,26 +1,32 @@
-// Fixed-size (power-of-two) pass kernels of the zero-aware padded FFT.
+// Fixed-size pass kernels of the zero-aware padded FFT.
 // Drop-in replacements for k_col / k_z_r2c / k_z_c2r (fft_passes.cuh) and
 // for the fused k_xconv / k_yconv2d / k_zinv_epi (solver.cu) when the line
-// length is a power of two between 4 and 4096.
+// length has compiled kernels (FX_SIZES).
 #pragma once
 #include "epilogue.cuh"
 #include "kernmul.cuh"
 #include "fft_fixed.cuh"
 #include "fft_passes.cuh"
 
+// Row pitch of an index-major tile: odd, so that rows a power of two apart
+// fall on different shared-memory banks.
+__host__ __device__ constexpr int odd_pitch(int lines) { return (lines % 2) ? lines : lines + 1; }
+
 // ---------------------------------------------------------------------
-// Column pass: TK adjacent columns x L, index-major tile (s[i*TK + l]).
+// Column pass: TK adjacent columns x L, index-major tile (s[i*TKP + l],
+// TKP = odd_pitch(TK)).
 // Stage 0 loads from global (rows >= n_in are zero), the last stage stores
 // to global (only rows < n_out).
 // ---------------------------------------------------------------------
 template <int L, int TK, int T, bool INV>
-__global__ void __launch_bounds__(T) k_col_fx(const float2* src, float2* dst, ColPass cp) {
+__device__ __forceinline__ void col_body(const float2* src, float2* dst, const ColPass& cp, int bx, int by) {
   __shared__ float2 tw[L];
   extern __shared__ float2 sm[];
   constexpr int NST = n_stages(L);
+  constexpr int TKP = odd_pitch(TK);
   load_twiddles<L, T>(tw, cp.f.tw, cp.f.tws);
-  const int c0 = blockIdx.x * TK;
-  const int64_t pbase = (int64_t)blockIdx.y * cp.plane_stride + c0;
+  const int c0 = bx * TK;
+  const int64_t pbase = (int64_t)by * cp.plane_stride + c0;
   const int nc = min(TK, cp.ncols - c0);
   const int64_t sti = cp.stride_i;
   const int n_in = cp.n_in, n_out = cp.n_out;
@@ -58,10 +64,10 @@ __global__ void __launch_bounds__(T) k_col_fx(const float2* src, float2* dst, Co
       int l, j;
       S0::lj(i, l, j);
 #pragma unroll
-      for (int q = 0; q < R0; q++) sm[S0::out_idx(j, q) * TK + l] = v[i][q];
+      for (int q = 0; q < R0; q++) sm[S0::out_idx(j, q) * TKP + l] = v[i][q];
     }
     __syncthreads();
-    MidStages<L, 1, NST - 1, TK, T, true, TK, 1, INV>::run(sm, tw);
+    MidStages<L, 1, NST - 1, TK, T, true, TKP, 1, INV>::run(sm, tw);
     constexpr int RL = INV ? inv_radix(L, NST - 1) : fwd_radix(L, NST - 1);
     constexpr int NSL = INV ? inv_span(L, NST - 1) : fwd_span(L, NST - 1);
     using SL = St<L, RL, NSL, TK, T, true>;
@@ -72,7 +78,7 @@ __global__ void __launch_bounds__(T) k_col_fx(const float2* src, float2* dst, Co
       int l, j;
       SL::lj(i, l, j);
 #pragma unroll
-      for (int q = 0; q < RL; q++) w[i][q] = sm[SL::in_idx(j, q) * TK + l];
+      for (int q = 0; q < RL; q++) w[i][q] = sm[SL::in_idx(j, q) * TKP + l];
       SL::twiddle(w[i], j, tw, INV);
       dft<RL>(w[i], INV);
 #pragma unroll
@@ -82,6 +88,11 @@ __global__ void __launch_bounds__(T) k_col_fx(const float2* src, float2* dst, Co
       }
     }
   }
+}
+
+template <int L, int TK, int T, bool INV>
+__global__ void __launch_bounds__(T) k_col_fx(const float2* src, float2* dst, ColPass cp) {
+  col_body<L, TK, T, INV>(src, dst, cp, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------
@@ -109,13 +120,14 @@ template <int L, int R, int NS, int TK, int T>
 using St3 = St<L, R, NS, TK, T, true>;  // (t, j) butterflies, components looped inside
 
 template <int L, int TK, int T, bool D2>
-__global__ void __launch_bounds__(T) k_conv_fx(ConvArgs a) {
+__device__ __forceinline__ void conv_body(const ConvArgs& a, int bx) {
   __shared__ float2 tw[L];
   extern __shared__ float2 sm[];
   constexpr int NST = n_stages(L);
   constexpr int NL = 3 * TK;
+  constexpr int NLP = odd_pitch(NL);
   load_twiddles<L, T>(tw, a.tw, a.tws);
-  const int col0 = blockIdx.x * TK;
+  const int col0 = bx * TK;
   const int nc = min(TK, a.ncols - col0);
   const int nd = a.n_data;
   // ---- forward stage 0 from global ----
@@ -158,11 +170,11 @@ __global__ void __launch_bounds__(T) k_conv_fx(ConvArgs a) {
         }
         dft<R0>(u[i][c], false);
 #pragma unroll
-        for (int q = 0; q < R0; q++) sm[S0::out_idx(j, q) * NL + c * TK + t] = u[i][c][q];
+        for (int q = 0; q < R0; q++) sm[S0::out_idx(j, q) * NLP + c * TK + t] = u[i][c][q];
       }
     }
     __syncthreads();
-    MidStages<L, 1, NST - 1, NL, T, true, NL, 1, false>::run(sm, tw);
+    MidStages<L, 1, NST - 1, NL, T, true, NLP, 1, false>::run(sm, tw);
 #pragma unroll
     for (int i = 0; i < SL::NB; i++) {
       if (!SL::valid(i)) continue;
@@ -171,7 +183,7 @@ __global__ void __launch_bounds__(T) k_conv_fx(ConvArgs a) {
 #pragma unroll
       for (int c = 0; c < 3; c++) {
 #pragma unroll
-        for (int q = 0; q < RL; q++) v[i][c][q] = sm[SL::in_idx(j, q) * NL + c * TK + t];
+        for (int q = 0; q < RL; q++) v[i][c][q] = sm[SL::in_idx(j, q) * NLP + c * TK + t];
         SL::twiddle(v[i][c], j, tw, false);
         dft<RL>(v[i][c], false);
       }
@@ -231,11 +243,11 @@ __global__ void __launch_bounds__(T) k_conv_fx(ConvArgs a) {
       for (int c = 0; c < 3; c++) {
         dft<RL>(v[i][c], true);
 #pragma unroll
-        for (int q = 0; q < RL; q++) sm[I0::out_idx(j, q) * NL + c * TK + t] = v[i][c][q];
+        for (int q = 0; q < RL; q++) sm[I0::out_idx(j, q) * NLP + c * TK + t] = v[i][c][q];
       }
     }
     __syncthreads();
-    MidStages<L, 1, NST - 1, NL, T, true, NL, 1, true>::run(sm, tw);
+    MidStages<L, 1, NST - 1, NL, T, true, NLP, 1, true>::run(sm, tw);
     constexpr int RI = inv_radix(L, NST - 1);
     constexpr int NSI = inv_span(L, NST - 1);
     using SI = St3<L, RI, NSI, TK, T>;
@@ -248,7 +260,7 @@ __global__ void __launch_bounds__(T) k_conv_fx(ConvArgs a) {
       for (int c = 0; c < 3; c++) {
         float2 w[RI];
 #pragma unroll
-        for (int q = 0; q < RI; q++) w[q] = sm[SI::in_idx(j, q) * NL + c * TK + t];
+        for (int q = 0; q < RI; q++) w[q] = sm[SI::in_idx(j, q) * NLP + c * TK + t];
         SI::twiddle(w, j, tw, true);
         dft<RI>(w, true);
 #pragma unroll
@@ -261,37 +273,53 @@ __global__ void __launch_bounds__(T) k_conv_fx(ConvArgs a) {
   }
 }
 
+template <int L, int TK, int T, bool D2>
+__global__ void __launch_bounds__(T) k_conv_fx(ConvArgs a) {
+  conv_body<L, TK, T, D2>(a, blockIdx.x);
+}
+
 // ---------------------------------------------------------------------
 // Z rows.  Tile index-major with an odd row pitch: element n of line l at
 // sm[n * SIP + l]; global accesses walk the row (coalesced), stages walk
 // the lines (conflict-free).
 // ---------------------------------------------------------------------
-__host__ __device__ constexpr int odd_pitch(int lines) { return (lines % 2) ? lines : lines + 1; }
 
 template <int M, int RT, int T, bool COMB>
-__global__ void __launch_bounds__(T) k_zr2c_fx(const float* __restrict__ src, float2* __restrict__ dst, ZPass z,
-                                               ZComb cb) {
+__device__ __forceinline__ void zr2c_body(const float* __restrict__ src, float2* __restrict__ dst, const ZPass& z,
+                                          const ZComb& cb, int vec2, int bx) {
   __shared__ float2 tw[M];
+  __shared__ int64_t roff_s[RT], soff_s[RT];
   extern __shared__ float2 sm[];
   constexpr int SIP = odd_pitch(RT);
   load_twiddles<M, T>(tw, z.f.tw, z.f.tws);
-  const int r0 = blockIdx.x * RT;
+  const int r0 = bx * RT;
   const int nl = min(RT, z.nrows - r0);
+  if (threadIdx.x < RT) {
+    int64_t ro = 0, so = 0;
+    if ((int)threadIdx.x < nl) zrow_offsets(z, r0 + threadIdx.x, &ro, &so);
+    roff_s[threadIdx.x] = ro;
+    soff_s[threadIdx.x] = so;
+  }
+  __syncthreads();
   const float dt = COMB ? *cb.dt : 0.f;
+  const int nreal = z.n_real;
+#pragma unroll 4
   for (int e = threadIdx.x; e < RT * M; e += T) {
-    int l = e / M, n = e - l * M;
+    int l = e / M, n = e % M;
     float a = 0.f, b = 0.f;
     if (l < nl) {
-      int64_t roff, soff;
-      zrow_offsets(z, r0 + l, &roff, &soff);
-      int i0 = 2 * n, i1 = 2 * n + 1;
+      int64_t roff = roff_s[l];
+      int i0 = 2 * n;
       if (COMB) {
-        if (i0 < z.n_real) { a = zcomb_value(cb, dt, roff + i0); cb.out[roff + i0] = a; }
-        if (i1 < z.n_real) { b = zcomb_value(cb, dt, roff + i1); cb.out[roff + i1] = b; }
+        if (i0 < nreal) { a = zcomb_value(cb, dt, roff + i0); cb.out[roff + i0] = a; }
+        if (i0 + 1 < nreal) { b = zcomb_value(cb, dt, roff + i0 + 1); cb.out[roff + i0 + 1] = b; }
+      } else if (vec2 && i0 + 1 < nreal) {
+        float2 p = __ldg(reinterpret_cast<const float2*>(src + roff + i0));
+        a = p.x;
+        b = p.y;
       } else {
-        const float* row = src + roff;
-        if (i0 < z.n_real) a = row[i0];
-        if (i1 < z.n_real) b = row[i1];
+        if (i0 < nreal) a = src[roff + i0];
+        if (i0 + 1 < nreal) b = src[roff + i0 + 1];
       }
     }
     sm[n * SIP + l] = make_float2(a, b);
@@ -300,16 +328,22 @@ __global__ void __launch_bounds__(T) k_zr2c_fx(const float* __restrict__ src, fl
   tile_fft_fixed<M, RT, T, true, SIP, 1, false>(sm, tw);
   for (int e = threadIdx.x; e < nl * (M + 1); e += T) {
     int l = e / (M + 1), k = e - l * (M + 1);
-    int64_t roff, soff;
-    zrow_offsets(z, r0 + l, &roff, &soff);
     float2 Zk = sm[(k == M ? 0 : k) * SIP + l];
     float2 Zm = sm[(k == 0 ? 0 : M - k) * SIP + l];
     float2 E = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
     float2 O = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
-    float2 w = __ldg(&z.twP[k]);
+    float2 w = tw[0];
+    if (k == M) w = make_float2(-1.f, 0.f);
+    else w = __ldg(&z.twP[k]);
     float2 wo = cmul_f(w, O);
-    dst[soff + k] = make_float2(E.x + wo.x, E.y + wo.y);
+    dst[soff_s[l] + k] = make_float2(E.x + wo.x, E.y + wo.y);
   }
+}
+
+template <int M, int RT, int T, bool COMB>
+__global__ void __launch_bounds__(T) k_zr2c_fx(const float* __restrict__ src, float2* __restrict__ dst, ZPass z,
+                                               ZComb cb, int vec2) {
+  zr2c_body<M, RT, T, COMB>(src, dst, z, cb, vec2, blockIdx.x);
 }
 
 // Z'_k = (X_k + conj X_{M-k}) + i (X_k - conj X_{M-k}) w^{-k}; X_0, X_M real
@@ -355,26 +389,45 @@ __global__ void __launch_bounds__(T) k_zc2r_fx(const float2* __restrict__ src, f
 }
 
 // Inverse Z of the three components of RT spatial rows + the solver epilogue.
+struct ZinvArgs {
+  const float2* S;
+  const float2* twz;
+  const float2* twP;
+  int P1, HZ;
+  int64_t CS;
+  int nrows;
+  EpiArgs ea;
+};
+
 template <int M, int RT, int T, int MODE>
-__global__ void __launch_bounds__(T) k_zinv_fx(const float2* __restrict__ S, const float2* __restrict__ twz,
-                                               const float2* __restrict__ twP, int P1, int HZ, int64_t CS, int nrows,
-                                               EpiArgs ea) {
+__device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
   __shared__ float2 tw[M];
+  __shared__ int64_t rbase_s[RT];
   extern __shared__ float2 sm[];
   constexpr int NL = 3 * RT;
   constexpr int SIP = odd_pitch(NL);
-  load_twiddles<M, T>(tw, twz, 2);
-  const int r0 = blockIdx.x * RT;
+  const float2* __restrict__ S = za.S;
+  const float2* __restrict__ twP = za.twP;
+  const int P1 = za.P1, HZ = za.HZ, nrows = za.nrows;
+  const int64_t CS = za.CS;
+  const EpiArgs& ea = za.ea;
+  load_twiddles<M, T>(tw, za.twz, 2);
+  const int r0 = bx * RT;
   const int nr = min(RT, nrows - r0);
   const int N1 = ea.N1, N2 = ea.N2;
+  if (threadIdx.x < RT) {
+    int gr = r0 + threadIdx.x;
+    int x = gr / N1, y = gr - x * N1;
+    rbase_s[threadIdx.x] = ((int64_t)x * P1 + y) * HZ;
+  }
+  __syncthreads();
+#pragma unroll 4
   for (int e = threadIdx.x; e < NL * M; e += T) {
-    int l = e / M, k = e - l * M;
+    int l = e / M, k = e % M;
     int r = l / 3, c = l - 3 * r;
     float2 v = make_float2(0.f, 0.f);
     if (r < nr) {
-      int gr = r0 + r;
-      int x = gr / N1, y = gr - x * N1;
-      const float2* row = S + c * CS + ((int64_t)x * P1 + y) * HZ;
+      const float2* row = S + c * CS + rbase_s[r];
       v = c2r_pre(row[k], row[M - k], k, M, twP);
     }
     sm[k * SIP + l] = v;
@@ -382,24 +435,48 @@ __global__ void __launch_bounds__(T) k_zinv_fx(const float2* __restrict__ S, con
   __syncthreads();
   tile_fft_fixed<M, NL, T, true, SIP, 1, true>(sm, tw);
   float lmax = 0.f;
-  for (int e = threadIdx.x; e < nr * N2; e += T) {
-    int r = e / N2, zz = e - r * N2;
-    int64_t g = (int64_t)(r0 + r) * N2 + zz;
-    const float2* base = sm + (zz >> 1) * SIP + 3 * r;
-    float hx = (zz & 1) ? base[0].y : base[0].x;
-    float hy = (zz & 1) ? base[1].y : base[1].x;
-    float hz = (zz & 1) ? base[2].y : base[2].x;
-    epi_cell<MODE>(ea, g, hx, hy, hz, lmax);
+  const int64_t g0 = (int64_t)r0 * N2;
+  if (N2 == M) {
+    // open boundary along Z: the row has exactly M cells
+    for (int e = threadIdx.x; e < nr * M; e += T) {
+      int r = e / M, zz = e % M;
+      const float2* base = sm + (zz >> 1) * SIP + 3 * r;
+      float hx = (zz & 1) ? base[0].y : base[0].x;
+      float hy = (zz & 1) ? base[1].y : base[1].x;
+      float hz = (zz & 1) ? base[2].y : base[2].x;
+      epi_cell<MODE>(ea, g0 + e, hx, hy, hz, lmax);
+    }
+  } else {
+    for (int e = threadIdx.x; e < nr * N2; e += T) {
+      int r = e / N2, zz = e - r * N2;
+      const float2* base = sm + (zz >> 1) * SIP + 3 * r;
+      float hx = (zz & 1) ? base[0].y : base[0].x;
+      float hy = (zz & 1) ? base[1].y : base[1].x;
+      float hz = (zz & 1) ? base[2].y : base[2].x;
+      epi_cell<MODE>(ea, g0 + e, hx, hy, hz, lmax);
+    }
   }
   epi_flush_max<MODE>(ea, lmax);
+}
+
+template <int M, int RT, int T, int MODE>
+__global__ void __launch_bounds__(T) k_zinv_fx(ZinvArgs za) {
+  zinv_body<M, RT, T, MODE>(za, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------
 // Launch-shape tables.  Every tile holds about 4096 complex values and
 // every thread about 16 (512 threads for the longest lines).
 // ---------------------------------------------------------------------
-#define FX_SIZES(X) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
-static inline bool fx_ok(int L) { return L >= 8 && L <= 4096 && (L & (L - 1)) == 0; }
+// line lengths with compiled kernels: 2^k (2..4096) and 3*2^k (6..3072)
+#define FX_SIZES(X)                                                                                      \
+  X(2) X(4) X(8) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096) X(6) X(12) X(24) X(48) \
+      X(96) X(192) X(384) X(768) X(1536) X(3072)
+static inline bool fx_ok(int L) {
+  if (L < 2) return false;
+  int m = L % 3 == 0 ? L / 3 : L;
+  return (m & (m - 1)) == 0 && L <= 4096;
+}
 
 __host__ __device__ constexpr int fx_col_tk(int L) { return L >= 4096 ? 1 : (4096 / L > 32 ? 32 : 4096 / L); }
 __host__ __device__ constexpr int fx_threads(int elems) {
@@ -410,7 +487,7 @@ template <int L, bool INV>
 cudaError_t fx_launch_col(const float2* src, float2* dst, const ColPass& cp, cudaStream_t st) {
   constexpr int TK = fx_col_tk(L);
   constexpr int T = fx_threads(TK * L);
-  size_t smem = sizeof(float2) * (size_t)TK * L;
+  size_t smem = sizeof(float2) * (size_t)odd_pitch(TK) * L;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_col_fx<L, TK, T, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 grid(div_up(cp.ncols, TK), cp.nplanes);
   k_col_fx<L, TK, T, INV><<<grid, T, smem, st>>>(src, dst, cp);
@@ -422,8 +499,9 @@ cudaError_t fx_launch_conv(const ConvArgs& a, cudaStream_t st) {
   constexpr int TK = L >= 2048 ? 1 : (1365 / L > 32 ? 32 : (1365 / L < 1 ? 1 : 1365 / L)) ;
   constexpr int TKP = TK >= 16 ? 16 : (TK >= 8 ? 8 : (TK >= 4 ? 4 : (TK >= 2 ? 2 : 1)));
   // one thread per (column, radix-8 butterfly): it owns the three components
-  constexpr int T = (TKP * L / 8) < 64 ? 64 : ((TKP * L / 8) > 512 ? 512 : (TKP * L / 8));
-  size_t smem = sizeof(float2) * (size_t)3 * TKP * L;
+  constexpr int NBF = TKP * (L / fwd_radix(L, n_stages(L) - 1));
+  constexpr int T = NBF < 64 ? 64 : (NBF > 512 ? 512 : ((NBF + 31) / 32) * 32);
+  size_t smem = sizeof(float2) * (size_t)odd_pitch(3 * TKP) * L;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_conv_fx<L, TKP, T, D2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_conv_fx<L, TKP, T, D2><<<div_up(a.ncols, TKP), T, smem, st>>>(a);
   return cudaGetLastError();
@@ -439,7 +517,9 @@ cudaError_t fx_launch_zr2c(const float* src, float2* dst, const ZPass& z, const 
   constexpr int T = fx_threads(RT * M);
   size_t smem = sizeof(float2) * (size_t)odd_pitch(RT) * M;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_zr2c_fx<M, RT, T, COMB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_zr2c_fx<M, RT, T, COMB><<<div_up(z.nrows, RT), T, smem, st>>>(src, dst, z, cb);
+  // 8-byte loads when every row starts at an even float offset
+  int vec2 = (z.ld_real % 2 == 0) && (z.comp_stride_real % 2 == 0) && (((uintptr_t)src & 7) == 0);
+  k_zr2c_fx<M, RT, T, COMB><<<div_up(z.nrows, RT), T, smem, st>>>(src, dst, z, cb, vec2);
   return cudaGetLastError();
 }
 
@@ -460,6 +540,15 @@ cudaError_t fx_launch_zinv(const float2* S, const float2* twz, const float2* twP
   constexpr int T = fx_threads(3 * RT * M);
   size_t smem = sizeof(float2) * (size_t)odd_pitch(3 * RT) * M;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_zinv_fx<M, RT, T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_zinv_fx<M, RT, T, MODE><<<div_up(nrows, RT), T, smem, st>>>(S, twz, twP, P1, HZ, CS, nrows, ea);
+  ZinvArgs za;
+  za.S = S;
+  za.twz = twz;
+  za.twP = twP;
+  za.P1 = P1;
+  za.HZ = HZ;
+  za.CS = CS;
+  za.nrows = nrows;
+  za.ea = ea;
+  k_zinv_fx<M, RT, T, MODE><<<div_up(nrows, RT), T, smem, st>>>(za);
   return cudaGetLastError();
 }

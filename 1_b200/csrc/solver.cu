@@ -31,6 +31,7 @@
 #include "epilogue.cuh"
 #include "kernmul.cuh"
 #include "fft_fixed_kernels.cuh"
+#include "solver_state.cuh"
 #include "../../include/mmx.h"
 
 static thread_local std::string g_err = "";
@@ -243,48 +244,6 @@ __global__ void k_maxabs(const float* __restrict__ a, int64_t n, float* out) {
 // ---------------------------------------------------------------------
 // Solver object
 // ---------------------------------------------------------------------
-struct PassTimer {
-  std::string name;
-  double ms = 0;
-  long long launches = 0;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
-};
-
-struct mmx_solver {
-  mmx_params p;
-  int N[3], P[3], HZ;
-  int64_t n;
-  int is2d;
-  BoxPlan bp;
-  float2* S = nullptr;
-  int64_t CS = 0;
-  float* kh = nullptr;
-  KernOct K;
-  float* m = nullptr;
-  float* t0 = nullptr;
-  float* m1 = nullptr;
-  float* scratch = nullptr;  // device scalars: [0] err, [1] torque, [2] dt
-  float* kb[RK_MAXS] = {nullptr};
-  float* mnew = nullptr;
-  // solver scalars (host mirror)
-  double time = 0;
-  float dt = 0;
-  float torque = 0, step_error = 0;
-  long long steps = 0;
-  int fsal_init = 0;
-  // tableau
-  int stages = 0, fsal = 0, adaptive = 0;
-  double errorder = 1;
-  float a[RK_MAXS][RK_MAXS], b[RK_MAXS], b2[RK_MAXS], c[RK_MAXS];
-  // graph
-  int use_graph = 0;
-  cudaGraphExec_t gexec = nullptr;
-  cudaStream_t gstream = nullptr;
-  // profiling
-  int profile = 0;
-  std::vector<PassTimer> timers;
-};
-
 static void set_tableau(mmx_solver* s) {
   memset(s->a, 0, sizeof(s->a));
   memset(s->b, 0, sizeof(s->b));
@@ -526,7 +485,7 @@ static cudaError_t conv_front(mmx_solver* s, const float* m, cudaStream_t st) {
   return e;
 }
 
-static EpiArgs base_args(mmx_solver* s) {
+EpiArgs solver_base_args(mmx_solver* s) {
   EpiArgs ea;
   memset(&ea, 0, sizeof(ea));
   ea.N1 = s->N[1];
@@ -543,16 +502,11 @@ static EpiArgs base_args(mmx_solver* s) {
 }
 
 // ------------------------------ steps ---------------------------------
-// Host float32 arithmetic (one rounding per operation; x86-64 SSE, no
-// contraction) for the scalars the Go driver computes in float32.
-static inline float f32_div(float a, float b) { volatile float r = a / b; return r; }
-static inline float f32_mul(float a, float b) { volatile float r = a * b; return r; }
-static inline float f32_add(float a, float b) { volatile float r = a + b; return r; }
 static cudaError_t heun_step(mmx_solver* s, cudaStream_t st) {
   // dtGilbert = dt / (1 + alpha^2)   (torque.go:49-51)
   float dtg = f32_div(s->dt, f32_add(1.f, f32_mul(s->p.alpha, s->p.alpha)));
   cudaError_t e;
-  EpiArgs ea = base_args(s);
+  EpiArgs ea = solver_base_args(s);
   ea.dtg = dtg;
   // predictor
   e = conv_front(s, s->m, st);
@@ -630,7 +584,7 @@ static cudaError_t rk_stage(mmx_solver* s, int i, cudaStream_t st, float* dt_dev
     }
   }
   if (e != cudaSuccess) return e;
-  EpiArgs ea = base_args(s);
+  EpiArgs ea = solver_base_args(s);
   ea.dtg = f32_div(1.f, f32_add(1.f, f32_mul(s->p.alpha, s->p.alpha)));  // Torque = DeltaM(dt=1)
   ea.m_in = src;
   ea.dt_dev = dt_dev;
@@ -696,7 +650,7 @@ __global__ void k_avg_finish(const double* __restrict__ acc, double n, float* __
   if (threadIdx.x < 3) out[threadIdx.x] = (float)(acc[threadIdx.x] / n);
 }
 
-static int grid_1d(int64_t n) {
+int solver_grid_1d(int64_t n) {
   int64_t b = (n + 255) / 256;
   int64_t cap = (int64_t)mmx_sm_count() * 8;
   return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
@@ -728,7 +682,7 @@ static int rk_step(mmx_solver* s, cudaStream_t st) {
           s->kb[last] = t;
         }
         MMX_TRY(cudaMemsetAsync(s->scratch + 1, 0, sizeof(float), st));
-        k_maxabs<<<grid_1d(3 * s->n), 256, 0, st>>>(s->kb[0], 3 * s->n, s->scratch + 1);
+        k_maxabs<<<solver_grid_1d(3 * s->n), 256, 0, st>>>(s->kb[0], 3 * s->n, s->scratch + 1);
         MMX_TRY(cudaGetLastError());
       } else {
         if (i == 0) MMX_TRY(cudaMemsetAsync(s->scratch + 1, 0, sizeof(float), st));
@@ -781,7 +735,7 @@ static int rk_step(mmx_solver* s, cudaStream_t st) {
     MMX_TRY(cudaMemcpyAsync(acc_dev, &accv, sizeof(int), cudaMemcpyHostToDevice, st));
   }
   // m <- normalize(m_high) if accepted, else normalize(m)   (rk.go:444)
-  k_finalize_accept<<<grid_1d(s->n), 256, 0, st>>>(s->m, s->mnew, s->n, acc_dev);
+  k_finalize_accept<<<solver_grid_1d(s->n), 256, 0, st>>>(s->m, s->mnew, s->n, acc_dev);
   MMX_TRY(cudaGetLastError());
   return MMX_OK;
 }
@@ -919,7 +873,7 @@ extern "C" int mmx_solver_create(const mmx_params* p, mmx_solver** out) {
         continue;
       }
       if (box_forward(&full, k6 + c * p3, spec, 0) != cudaSuccess) rc = MMX_ERR_CUDA;
-      k_extract_octant<<<grid_1d(ocs), 256>>>(spec, s->kh + c * ocs, O0, O1, s->P[1], s->HZ, norm);
+      k_extract_octant<<<solver_grid_1d(ocs), 256>>>(spec, s->kh + c * ocs, O0, O1, s->P[1], s->HZ, norm);
     }
     cudaError_t ce = cudaDeviceSynchronize();
     cudaFree(k6);
@@ -964,7 +918,7 @@ extern "C" int mmx_solver_get_m(mmx_solver* s, float* m, int on_host, cudaStream
 
 extern "C" int mmx_solver_normalize(mmx_solver* s, cudaStream_t st) {
   if (!s) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
-  k_normalize3<<<grid_1d(s->n), 256, 0, st>>>(s->m, s->n);
+  k_normalize3<<<solver_grid_1d(s->n), 256, 0, st>>>(s->m, s->n);
   MMX_TRY(cudaGetLastError());
   return MMX_OK;
 }
@@ -973,7 +927,7 @@ extern "C" int mmx_solver_field(mmx_solver* s, const float* m, float* h, cudaStr
   if (!s || !m || !h) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
   cudaError_t e = conv_front(s, m, st);
   if (e == cudaSuccess) {
-    EpiArgs ea = base_args(s);
+    EpiArgs ea = solver_base_args(s);
     ea.m_in = m;
     ea.out0 = h;
     e = launch_zinv<EPI_FIELD>(s, ea, st);
@@ -1030,7 +984,7 @@ extern "C" int mmx_solver_avg_m(mmx_solver* s, float* out3, int on_host, cudaStr
   double* acc = reinterpret_cast<double*>(s->scratch + 8);
   float* res = s->scratch + 4;
   MMX_TRY(cudaMemsetAsync(acc, 0, 3 * sizeof(double), st));
-  k_sum3<<<grid_1d(s->n), 256, 0, st>>>(s->m, s->n, acc);
+  k_sum3<<<solver_grid_1d(s->n), 256, 0, st>>>(s->m, s->n, acc);
   MMX_TRY(cudaGetLastError());
   k_avg_finish<<<1, 32, 0, st>>>(acc, (double)s->n, on_host ? res : out3);
   MMX_TRY(cudaGetLastError());
@@ -1057,6 +1011,7 @@ extern "C" int mmx_solver_set_hext(mmx_solver* s, const float hext[3]) {
 }
 
 extern "C" float* mmx_solver_m_device(mmx_solver* s) { return s ? s->m : nullptr; }
+extern "C" float* mmx_solver_torque_device(mmx_solver* s) { return s ? s->scratch + 1 : nullptr; }
 
 extern "C" int mmx_solver_use_graph(mmx_solver* s, int on) {
   if (!s) { mmx_set_error("null argument"); return MMX_ERR_ARG; }

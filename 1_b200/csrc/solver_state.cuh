@@ -1,0 +1,63 @@
+// State of the fused solver (mmx_solver), shared by the single-instance
+// solver (solver.cu) and the batched form (batch.cu).
+#pragma once
+#include <string>
+#include <vector>
+
+#include "epilogue.cuh"
+#include "fft_passes.cuh"
+#include "kernmul.cuh"
+#include "../../include/mmx.h"
+
+struct PassTimer {
+  std::string name;
+  double ms = 0;
+  long long launches = 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+};
+
+struct mmx_solver {
+  mmx_params p;
+  int N[3], P[3], HZ;
+  int64_t n;
+  int is2d;
+  BoxPlan bp;
+  float2* S = nullptr;
+  int64_t CS = 0;
+  float* kh = nullptr;
+  KernOct K;
+  float* m = nullptr;
+  float* t0 = nullptr;
+  float* m1 = nullptr;
+  float* scratch = nullptr;  // device scalars: [0] err, [1] torque, [2] dt
+  float* kb[RK_MAXS] = {nullptr};
+  float* mnew = nullptr;
+  // solver scalars (host mirror)
+  double time = 0;
+  float dt = 0;
+  float torque = 0, step_error = 0;
+  long long steps = 0;
+  int fsal_init = 0;
+  // tableau
+  int stages = 0, fsal = 0, adaptive = 0;
+  double errorder = 1;
+  float a[RK_MAXS][RK_MAXS], b[RK_MAXS], b2[RK_MAXS], c[RK_MAXS];
+  // graph
+  int use_graph = 0;
+  cudaGraphExec_t gexec = nullptr;
+  cudaStream_t gstream = nullptr;
+  // profiling
+  int profile = 0;
+  std::vector<PassTimer> timers;
+};
+
+// Host float32 arithmetic (one rounding per operation; x86-64 SSE, no
+// contraction) for the scalars the Go driver computes in float32.
+static inline float f32_div(float a, float b) { volatile float r = a / b; return r; }
+static inline float f32_mul(float a, float b) { volatile float r = a * b; return r; }
+static inline float f32_add(float a, float b) { volatile float r = a + b; return r; }
+
+// Fills the per-cell epilogue arguments common to every stage.
+EpiArgs solver_base_args(mmx_solver* s);
+// Device launch grid for a 1D element-wise kernel over n items.
+int solver_grid_1d(int64_t n);

@@ -40,6 +40,10 @@ WORKLOADS = {
         grid=(128, 32, 1), cell=(3.90625e-9, 3.90625e-9, 3e-9), msat=8.0e5, aexch=1.3e-11, alpha=0.02,
         bext=(-24.6e-3, 4.3e-3, 0.0), solver="heun", dt=1e-14, seed=1, init="tilted"),
 }
+BATCH_WORKLOADS = {
+    # BASELINE batching configuration: 256 instances, RK4, fixed dt 5e-15 s
+    "batch-fp32-rk4-256": dict(count=256, seed=4, solver="rk4", dt=5e-15),
+}
 DEFAULT = "plain-fp32-heun-256x256x32"
 
 
@@ -172,6 +176,47 @@ def cpu_baseline(w, steps_budget_s=20.0):
     return {"value": n * done / el, "unit": "cell-steps/s", "cores": O.num_threads(), "kind": "port",
             "sample": "%d whole-grid Heun steps of %s after 1 untimed step (setup incl. kernel %.1f s untimed)" % (
                 done, "x".join(map(str, w["grid"])), setup)}
+
+
+def run_batch(args, name):
+    """The batched form: many uneven-size instances, one launch per pass and
+    line length, one CUDA graph per step."""
+    import torch
+    eng = importlib.import_module("1_b200")
+    bw = BATCH_WORKLOADS[name]
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    cfgs = eng.batch_config(bw["count"], seed=bw["seed"], solver=bw["solver"], dt=bw["dt"])
+    t0 = time.perf_counter()
+    b = eng.Batch([eng.mmx_params(**c) for c in cfgs])
+    setup = time.perf_counter() - t0
+    for i, (inst, c) in enumerate(zip(b.instances, cfgs)):
+        inst.set_m(seeded_m(c["grid"], 1000 + i, "random"))
+        inst.normalize()
+    info = b.size()
+    stream = torch.cuda.Stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    b.use_graph(True)
+    b.step(args.warmup, sh)
+    torch.cuda.synchronize()
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.step(args.steps, sh)
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    cells = info["cells"]
+    line = {"metric": "cell-steps/s", "value": cells * args.steps / (ms / 1e3), "unit": "cell-steps/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": name, "instances": info["count"], "cells": cells, "solver": bw["solver"],
+                       "dt_s": bw["dt"], "launches_per_step": info["launches_per_step"],
+                       "setup_s": setup},
+            "instance_steps_per_s": info["count"] * args.steps / (ms / 1e3),
+            "gpu_launches": info["launches_per_step"] * args.steps, "clocks": clk}
+    b.close()
+    print(json.dumps(line), flush=True)
 
 
 def run_reference(args, w, name):
@@ -316,9 +361,12 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.workload in BATCH_WORKLOADS:
+        run_batch(args, args.workload)
+        return
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, w, args.workload)

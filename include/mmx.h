@@ -105,6 +105,8 @@ int mmx_solver_state(mmx_solver* s, double* time, float* dt, float* max_torque, 
 int mmx_solver_set_hext(mmx_solver* s, const float hext[3]);
 /* Device pointer of the resident magnetisation (3*N floats). */
 float* mmx_solver_m_device(mmx_solver* s);
+/* Device address of the solver's last maximum torque (one float). */
+float* mmx_solver_torque_device(mmx_solver* s);
 
 /* Capture one step in a CUDA graph and replay it (fixed-step solvers). */
 int mmx_solver_use_graph(mmx_solver* s, int on);
@@ -114,6 +116,26 @@ int mmx_solver_use_graph(mmx_solver* s, int on);
  * returns the accumulated milliseconds and launch counts per pass name. */
 int mmx_solver_profile(mmx_solver* s, int on);
 int mmx_solver_pass_times(mmx_solver* s, int max, char (*names)[32], double* ms, long long* launches, int* n);
+
+/* Batched form: 'count' independent instances (sizes, materials and fields
+ * may all differ) advanced together with a fixed-step Heun or RK4 solver.
+ * Each field-evaluation pass is ONE launch per distinct line length over
+ * every instance that has it; with use_graph a whole step is one CUDA graph.
+ * Instance i is a full solver: set / read its m with mmx_solver_set_m /
+ * mmx_solver_get_m on mmx_batch_instance(b, i).  Padded sizes must be 2^k
+ * or 3*2^k (<= 4096). */
+typedef struct mmx_batch mmx_batch;
+int mmx_batch_create(const mmx_params* p, int count, mmx_batch** out);
+/* A batch over solvers the caller owns (they outlive the batch); used by a
+ * serving loop to regroup resident solves as they join and leave.  After a
+ * step of an RK4 batch, each solver's mmx_solver_torque_device slot holds
+ * the maximum |k0| (torque) of that step's first stage. */
+int mmx_batch_create_from(mmx_solver* const* solvers, int count, mmx_batch** out);
+int mmx_batch_destroy(mmx_batch* b);
+mmx_solver* mmx_batch_instance(mmx_batch* b, int i);
+int mmx_batch_size(mmx_batch* b, int* count, long long* cells, int* launches_per_step);
+int mmx_batch_step(mmx_batch* b, int nsteps, cudaStream_t stream);
+int mmx_batch_use_graph(mmx_batch* b, int on);
 
 /* Allocation-free reduction.  No counterpart in the reference: a variant of
  * gpu_reduce (same operations, 1 add, 2 max, 3 max |x|, 4 min, 5 sum |x|)

@@ -12,6 +12,7 @@ Nothing here falls back to a CPU path: if the CUDA library is missing the
 import fails with a message naming the build step.
 """
 import ctypes
+import time
 import os
 import subprocess
 
@@ -64,6 +65,40 @@ class MmxParams(ctypes.Structure):
         ("exch_type", ctypes.c_int),
         ("faithful", ctypes.c_int),
         ("accuracy", ctypes.c_int),
+    ]
+
+
+class MmxRequest(ctypes.Structure):
+    _fields_ = [
+        ("params", MmxParams),
+        ("m0", ctypes.c_void_p),
+        ("npoints", ctypes.c_int),
+        ("hext_points", ctypes.c_void_p),
+        ("max_torque", ctypes.c_float),
+        ("max_steps", ctypes.c_longlong),
+    ]
+
+
+class MmxServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("hbm_budget", ctypes.c_size_t),
+        ("max_active", ctypes.c_int),
+        ("check_every", ctypes.c_int),
+        ("batched", ctypes.c_int),
+        ("keep_m", ctypes.c_int),
+    ]
+
+
+class MmxResult(ctypes.Structure):
+    _fields_ = [
+        ("state", ctypes.c_int),
+        ("converged", ctypes.c_int),
+        ("steps", ctypes.c_longlong),
+        ("points_done", ctypes.c_int),
+        ("t_submit", ctypes.c_double),
+        ("t_admit", ctypes.c_double),
+        ("t_done", ctypes.c_double),
+        ("footprint", ctypes.c_size_t),
     ]
 
 
@@ -198,6 +233,21 @@ MMX = {
                                       ctypes.POINTER(ctypes.c_int)]),
     "mmx_batch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "mmx_batch_use_graph": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "mmx_batch_create_from": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "mmx_batch_torques": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "mmx_solver_torque_device": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "mmx_server_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "mmx_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "mmx_server_footprint": (ctypes.c_int, [ctypes.POINTER(MmxParams), ctypes.POINTER(ctypes.c_size_t)]),
+    "mmx_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
+    "mmx_server_pump": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "mmx_server_result": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p]),
+    "mmx_server_result_m": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p]),
+    "mmx_server_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong]),
+    "mmx_server_clock": (ctypes.c_double, [ctypes.c_void_p]),
+    "mmx_server_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t),
+                                        ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "mmx_reduce_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                          ctypes.c_void_p]),
     "mmx_face_kernel6": (ctypes.c_int, [c_int_p, c_int_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int,
@@ -463,6 +513,213 @@ def batch_config(count, seed=4, cell=3e-9, solver="rk4", dt=5e-15):
         out.append(dict(grid=(nx, ny, nz), cell=(cell, cell, cell), msat=ms, aexch=a, alpha=alpha,
                         bext=tuple(float(x) for x in bmag * d), solver=solver, dt=dt))
     return out
+
+
+# --------------------------------------------------------------------------
+# Serving form (mmx_server_*)
+# --------------------------------------------------------------------------
+REQ_STATES = {0: "queued", 1: "active", 2: "done", 3: "failed"}
+
+
+def footprint(params):
+    """Device bytes a resident solve with these parameters holds."""
+    b = ctypes.c_size_t()
+    _check(lib().mmx_server_footprint(ctypes.byref(params), ctypes.byref(b)))
+    return b.value
+
+
+class Server:
+    """The request loop with continuous batching (batched=True) or one solve
+    at a time on the single-instance solver (batched=False)."""
+
+    def __init__(self, batched=True, check_every=100, hbm_budget=0, max_active=0, keep_m=False, stream=None):
+        c = MmxServerConfig()
+        c.hbm_budget, c.max_active, c.check_every = int(hbm_budget), int(max_active), int(check_every)
+        c.batched, c.keep_m = 1 if batched else 0, 1 if keep_m else 0
+        self.h = ctypes.c_void_p()
+        _check(lib().mmx_server_create(ctypes.byref(c), stream, ctypes.byref(self.h)))
+        self.npoints = {}
+        self.sizes = {}
+
+    def close(self):
+        if self.h:
+            lib().mmx_server_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, params, m0, fields=None, max_torque=1e-4, max_steps=0):
+        """Queues one solve.  m0: internal [3][X][Y][Z] float32; fields: None
+        (relax under params.hext) or an (npoints, 3) array of internal fields."""
+        r = MmxRequest()
+        r.params = params
+        m0 = np.ascontiguousarray(m0, dtype=np.float32)
+        r.m0 = m0.ctypes.data
+        f = None
+        if fields is None:
+            r.npoints = 1
+        else:
+            f = np.ascontiguousarray(fields, dtype=np.float32).reshape(-1, 3)
+            r.npoints = f.shape[0]
+            r.hext_points = f.ctypes.data
+        r.max_torque = max_torque
+        r.max_steps = max_steps
+        rid = ctypes.c_longlong()
+        _check(lib().mmx_server_submit(self.h, ctypes.byref(r), ctypes.byref(rid)))
+        self.npoints[rid.value] = r.npoints
+        self.sizes[rid.value] = tuple(params.size)
+        return rid.value
+
+    def pump(self):
+        a, q = ctypes.c_int(), ctypes.c_int()
+        _check(lib().mmx_server_pump(self.h, ctypes.byref(a), ctypes.byref(q)))
+        return a.value, q.value
+
+    def result(self, rid):
+        res = MmxResult()
+        npts = self.npoints[rid]
+        avg = np.zeros((npts, 3), np.float32)
+        ps = np.zeros(npts, np.int64)
+        _check(lib().mmx_server_result(self.h, rid, ctypes.byref(res), avg.ctypes.data, ps.ctypes.data))
+        k = res.points_done
+        return dict(state=REQ_STATES[res.state], converged=bool(res.converged), steps=res.steps, points_done=k,
+                    t_submit=res.t_submit, t_admit=res.t_admit, t_done=res.t_done, footprint=res.footprint,
+                    avg_m=avg[:k], point_steps=ps[:k])
+
+    def result_m(self, rid):
+        N = self.sizes[rid]
+        m = np.empty((3,) + N, np.float32)
+        _check(lib().mmx_server_result_m(self.h, rid, m.ctypes.data))
+        return m
+
+    def release(self, rid):
+        _check(lib().mmx_server_release(self.h, rid))
+        self.npoints.pop(rid, None)
+        self.sizes.pop(rid, None)
+
+    def clock(self):
+        return lib().mmx_server_clock(self.h)
+
+    def stats(self):
+        u, c, g = ctypes.c_size_t(), ctypes.c_longlong(), ctypes.c_longlong()
+        _check(lib().mmx_server_stats(self.h, ctypes.byref(u), ctypes.byref(c), ctypes.byref(g)))
+        return dict(used_bytes=u.value, chunks=c.value, regroups=g.value)
+
+
+def sweep_fields(msat, aexch, b0, b1, points):
+    """Internal fields of a sweep from b0 to b1 (user x,y,z, tesla) in
+    points-1 intervals: b = b0 + (b1-b0)*float32(i)/float32(points-1) in
+    float32 (simhysteresis.go:18-24), then the ApplyStatic conversion to
+    internal units and axes (simfield.go:87-98)."""
+    u = units(msat, aexch)
+    steps = f32(points - 1)
+    out = np.zeros((points, 3), np.float32)
+    for i in range(points):
+        frac = f32(f32(i) / steps)
+        for d in range(3):
+            b = f32(f32(b0[d]) + f32(f32(f32(b1[d]) - f32(b0[d])) * frac))
+            out[i, 2 - d] = f32(b / u["field"])
+    return out
+
+
+def serve_stream(count, seed=5, rate=200.0, cell=3e-9, dt=1e-13, sweep_points=21, sweep_fraction=0.5,
+                 bmax=0.1):
+    """The serving workload: a Poisson stream (rate requests/s) of
+    relaxations (alpha = 1, under a uniform field drawn as in the batch
+    configuration) and field sweeps (alpha = 1, B along user x from -bmax to
+    +bmax tesla in sweep_points points), sizes and materials drawn as in
+    batch_config, random unit m per cell.  Per request, in order: the
+    inter-arrival gap, the kind, then the batch_config draws; m comes from
+    its own generator seeded (seed, index).  Returns dicts with 'arrival'
+    (s), 'kind', 'cfg' (user-level) and 'fields' (None or internal)."""
+    rng = np.random.default_rng(seed)
+    sizes = [32, 48, 64, 96, 128, 192, 256]
+    t = 0.0
+    out = []
+    for i in range(count):
+        t += float(rng.exponential(1.0 / rate))
+        sweep = bool(rng.uniform() < sweep_fraction)
+        nx = int(rng.choice(sizes))
+        ny = int(rng.choice(sizes))
+        nz = int(rng.choice([1, 2, 4]))
+        ms = float(rng.uniform(4e5, 1.4e6))
+        a = float(rng.uniform(5e-12, 2e-11))
+        float(rng.uniform(0.01, 0.5))  # the batch alpha draw, kept for the draw order; relaxations use alpha = 1
+        d = rng.standard_normal(3)
+        d = d / np.linalg.norm(d)
+        bmag = float(rng.uniform(0.0, bmax))
+        cfg = dict(grid=(nx, ny, nz), cell=(cell, cell, cell), msat=ms, aexch=a, alpha=1.0,
+                   bext=(0.0, 0.0, 0.0) if sweep else tuple(float(x) for x in bmag * d), solver="rk4", dt=dt)
+        fields = sweep_fields(ms, a, (-bmax, 0.0, 0.0), (bmax, 0.0, 0.0), sweep_points) if sweep else None
+        if sweep:
+            cfg["bext"] = (-bmax, 0.0, 0.0)
+        out.append(dict(index=i, arrival=t, kind="sweep" if sweep else "relax", cfg=cfg, fields=fields,
+                        m_seed=(seed, i)))
+    return out
+
+
+def stream_m0(req):
+    """Random unit m per cell (internal layout) of a serve_stream request."""
+    nx, ny, nz = req["cfg"]["grid"]
+    g = np.random.default_rng(list(req["m_seed"]))
+    u = g.standard_normal((3, nz, ny, nx))
+    u /= np.sqrt((u * u).sum(axis=0, keepdims=True))
+    return np.ascontiguousarray(u[::-1].astype(np.float32))
+
+
+def partition_requests(reqs, world):
+    """Rank of every request when the stream is spread over 'world' GPUs:
+    in arrival order, each request goes to the rank with the least device
+    bytes x field points assigned so far (ties to the lowest rank).  Every
+    rank computes the same partition; there is no data exchange."""
+    load = [0] * world
+    out = []
+    for r in sorted(reqs, key=lambda q: q["arrival"]):
+        w = footprint(mmx_params(**r["cfg"])) * (1 if r["fields"] is None else len(r["fields"]))
+        k = min(range(world), key=lambda i: (load[i], i))
+        load[k] += w
+        out.append((r["index"], k))
+    ranks = dict(out)
+    return [ranks[r["index"]] for r in reqs]
+
+
+def run_stream(server, reqs, realtime=True, max_torque=1e-4, max_steps=0, poll=0.0005):
+    """Drives a Server with the requests' arrival times: each request is
+    submitted once the server clock passes its arrival (all at once when
+    realtime is False) and the loop pumps while work is resident or queued.
+    Returns per-request results with latency = completion - arrival."""
+    t0 = server.clock()
+    pending = sorted(reqs, key=lambda r: r["arrival"])
+    ids = {}
+    k = 0
+    while True:
+        now = server.clock() - t0
+        while k < len(pending) and (not realtime or pending[k]["arrival"] <= now):
+            r = pending[k]
+            p = mmx_params(**r["cfg"])
+            ids[server.submit(p, stream_m0(r), r["fields"], max_torque, max_steps)] = r
+            k += 1
+        active, queued = server.pump()
+        if active == 0 and queued == 0:
+            if k == len(pending):
+                break
+            wait = pending[k]["arrival"] - (server.clock() - t0)
+            if wait > 0:
+                time.sleep(min(wait, poll) if poll else wait)
+    out = []
+    for rid, r in ids.items():
+        res = server.result(rid)
+        res["id"] = rid
+        res["index"] = r["index"]
+        res["kind"] = r["kind"]
+        res["arrival"] = r["arrival"] if realtime else 0.0
+        res["latency"] = res["t_done"] - t0 - res["arrival"]
+        out.append(res)
+    return sorted(out, key=lambda x: x["index"])
 
 
 def face_kernel6_device(P, periodic, cellsize, exch6=True, accuracy=8, out_ptr=None, stream=None):

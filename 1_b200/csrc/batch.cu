@@ -109,6 +109,7 @@ struct mmx_batch {
   long long cells = 0;
   int launches_per_step = 0;
   float** torque_ptrs = nullptr;  // RK4: per-instance max |k0| slots, cleared each step
+  float* gather = nullptr;        // device staging of the gathered torques
 };
 
 __global__ void kb_clear(float** p, int n) {
@@ -660,6 +661,26 @@ extern "C" int mmx_batch_step(mmx_batch* b, int nsteps, cudaStream_t st) {
       s->steps++;
     }
   }
+  return MMX_OK;
+}
+
+__global__ void kb_gather(float* const* __restrict__ p, int n, float* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = *p[i];
+}
+
+extern "C" int mmx_batch_torques(mmx_batch* b, float* out, int on_host, cudaStream_t st) {
+  if (!b || !out) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  if (!b->torque_ptrs) { mmx_set_error("torques are recorded by RK4 batches only"); return MMX_ERR_STATE; }
+  int n = (int)b->inst.size();
+  if (!b->gather) {
+    if (cudaMalloc(&b->gather, sizeof(float) * n) != cudaSuccess) { mmx_set_error("out of device memory"); return MMX_ERR_MEM; }
+    b->owned.push_back(b->gather);
+  }
+  float* dst = on_host ? b->gather : out;
+  kb_gather<<<(n + 255) / 256, 256, 0, st>>>(b->torque_ptrs, n, dst);
+  MMX_TRY(cudaGetLastError());
+  if (on_host) MMX_TRY(cudaMemcpyAsync(out, b->gather, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
   return MMX_OK;
 }
 

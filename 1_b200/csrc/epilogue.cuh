@@ -34,11 +34,52 @@ struct EpiArgs {
 };
 
 
+// Per-cell inputs an epilogue reads besides the field: m at which the field
+// was evaluated, and for Heun's corrector t0 and m (aux0, aux1), for an RK
+// stage the step-start m (aux0).  Loaded ahead of the transform so that
+// their latency overlaps it.
+template <int MODE>
+struct EpiIn {
+  float m[3];
+  float a0[(MODE == EPI_HEUN2 || MODE == EPI_RK) ? 3 : 1];
+  float a1[MODE == EPI_HEUN2 ? 3 : 1];
+};
+
+template <int MODE>
+__device__ __forceinline__ void epi_load(const EpiArgs& ea, int64_t g, EpiIn<MODE>& in) {
+  const int64_t n = ea.n;
+  in.m[0] = ea.m_in[g];
+  in.m[1] = ea.m_in[n + g];
+  in.m[2] = ea.m_in[2 * n + g];
+  if (MODE == EPI_HEUN2 || MODE == EPI_RK) {
+    in.a0[0] = ea.aux0[g];
+    in.a0[1] = ea.aux0[n + g];
+    in.a0[2] = ea.aux0[2 * n + g];
+  }
+  if (MODE == EPI_HEUN2) {
+    in.a1[0] = ea.aux1[g];
+    in.a1[1] = ea.aux1[n + g];
+    in.a1[2] = ea.aux1[2 * n + g];
+  }
+}
+
+template <int MODE>
+__device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float hx, float hy, float hz,
+                                            const EpiIn<MODE>& in, float& lmax);
+
 // cell g (index into one component), field (hx,hy,hz) from the convolution
 template <int MODE>
 __device__ __forceinline__ void epi_cell(const EpiArgs& ea, int64_t g, float hx, float hy, float hz, float& lmax) {
+  EpiIn<MODE> in;
+  epi_load<MODE>(ea, g, in);
+  epi_cell_in<MODE>(ea, g, hx, hy, hz, in, lmax);
+}
+
+template <int MODE>
+__device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float hx, float hy, float hz,
+                                            const EpiIn<MODE>& in, float& lmax) {
     const int64_t n = ea.n;
-    float mx = ea.m_in[g], my = ea.m_in[n + g], mz = ea.m_in[2 * n + g];
+    float mx = in.m[0], my = in.m[1], mz = in.m[2];
     llg_local(ea.lf, mx, my, mz, hx, hy, hz);
     if (MODE == EPI_FIELD) {
       ea.out0[g] = hx;
@@ -64,10 +105,10 @@ __device__ __forceinline__ void epi_cell(const EpiArgs& ea, int64_t g, float hx,
       ea.out1[2 * n + g] = ez;
     } else if (MODE == EPI_HEUN2) {
       // t = 0.5 t1 + 0.5 t0; m = normalize(m + t)   (adaptive_heun.go:148-154)
-      float tx = FA(FM(0.5f, hx), FM(0.5f, ea.aux0[g]));
-      float ty = FA(FM(0.5f, hy), FM(0.5f, ea.aux0[n + g]));
-      float tz = FA(FM(0.5f, hz), FM(0.5f, ea.aux0[2 * n + g]));
-      float nx = FA(ea.aux1[g], tx), ny = FA(ea.aux1[n + g], ty), nz = FA(ea.aux1[2 * n + g], tz);
+      float tx = FA(FM(0.5f, hx), FM(0.5f, in.a0[0]));
+      float ty = FA(FM(0.5f, hy), FM(0.5f, in.a0[1]));
+      float tz = FA(FM(0.5f, hz), FM(0.5f, in.a0[2]));
+      float nx = FA(in.a1[0], tx), ny = FA(in.a1[1], ty), nz = FA(in.a1[2], tz);
       llg_normalize(nx, ny, nz);
       ea.out0[g] = nx;
       ea.out0[n + g] = ny;
@@ -86,8 +127,8 @@ __device__ __forceinline__ void epi_cell(const EpiArgs& ea, int64_t g, float hx,
       kd[n + g] = ky;
       kd[2 * n + g] = kz;
       const float dt = *ea.dt_dev;
-      const float* m0 = ea.aux0;  // step start magnetisation
-      float q[3] = {m0[g], m0[n + g], m0[2 * n + g]};
+      // in.a0: the step-start magnetisation
+      float q[3] = {in.a0[0], in.a0[1], in.a0[2]};
       // next stage input (or m_high): m0 + sum_j (dt a_j) k_j, j in order
 #pragma unroll
       for (int j = 0; j < RK_MAXS; j++) {
@@ -103,7 +144,7 @@ __device__ __forceinline__ void epi_cell(const EpiArgs& ea, int64_t g, float hx,
         q[2] = FA(q[2], FM(c, k2));
       }
       if (ea.rk.final_stage && ea.rk.adaptive) {
-        float lo[3] = {m0[g], m0[n + g], m0[2 * n + g]};
+        float lo[3] = {in.a0[0], in.a0[1], in.a0[2]};
 #pragma unroll
         for (int j = 0; j < RK_MAXS; j++) {
           if (j >= ea.rk.nk) break;

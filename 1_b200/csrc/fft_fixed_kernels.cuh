@@ -432,21 +432,34 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
     }
     sm[k * SIP + l] = v;
   }
-  __syncthreads();
-  tile_fft_fixed<M, NL, T, true, SIP, 1, true>(sm, tw);
   float lmax = 0.f;
   const int64_t g0 = (int64_t)r0 * N2;
   if (N2 == M) {
-    // open boundary along Z: the row has exactly M cells
-    for (int e = threadIdx.x; e < nr * M; e += T) {
+    // open boundary along Z: the row has exactly M cells.  The epilogue's
+    // per-cell inputs are loaded before the transform.
+    constexpr int CPT = (RT * M + T - 1) / T;
+    EpiIn<MODE> in[CPT];
+#pragma unroll
+    for (int i = 0; i < CPT; i++) {
+      int e = threadIdx.x + i * T;
+      if (e < nr * M) epi_load<MODE>(ea, g0 + e, in[i]);
+    }
+    __syncthreads();
+    tile_fft_fixed<M, NL, T, true, SIP, 1, true>(sm, tw);
+#pragma unroll
+    for (int i = 0; i < CPT; i++) {
+      int e = threadIdx.x + i * T;
+      if (e >= nr * M) continue;
       int r = e / M, zz = e % M;
       const float2* base = sm + (zz >> 1) * SIP + 3 * r;
       float hx = (zz & 1) ? base[0].y : base[0].x;
       float hy = (zz & 1) ? base[1].y : base[1].x;
       float hz = (zz & 1) ? base[2].y : base[2].x;
-      epi_cell<MODE>(ea, g0 + e, hx, hy, hz, lmax);
+      epi_cell_in<MODE>(ea, g0 + e, hx, hy, hz, in[i], lmax);
     }
   } else {
+    __syncthreads();
+    tile_fft_fixed<M, NL, T, true, SIP, 1, true>(sm, tw);
     for (int e = threadIdx.x; e < nr * N2; e += T) {
       int r = e / N2, zz = e - r * N2;
       const float2* base = sm + (zz >> 1) * SIP + 3 * r;
@@ -478,7 +491,12 @@ static inline bool fx_ok(int L) {
   return (m & (m - 1)) == 0 && L <= 4096;
 }
 
-__host__ __device__ constexpr int fx_col_tk(int L) { return L >= 4096 ? 1 : (4096 / L > 32 ? 32 : 4096 / L); }
+// Columns per tile: at least 16 up to L = 512 so that a half-warp's 8-byte
+// accesses cover one 128-byte row of the tile (no shared-memory bank
+// conflicts) and global rows are read in 128-byte pieces.
+__host__ __device__ constexpr int fx_col_tk(int L) {
+  return L >= 4096 ? 1 : L >= 1024 ? 4096 / L : (4096 / L < 16 ? 16 : (4096 / L > 32 ? 32 : 4096 / L));
+}
 __host__ __device__ constexpr int fx_threads(int elems) {
   return elems / 16 < 64 ? 64 : (elems / 16 > 512 ? 512 : ((elems / 16 + 31) / 32) * 32);
 }

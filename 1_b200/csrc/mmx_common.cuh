@@ -48,6 +48,13 @@ enum {
     }                                          \
   } while (0)
 
+// Propagates a non-zero MMX_* status of an mmx_* call.
+#define MMX_CHECK_RC(call)       \
+  do {                           \
+    int rc_ = (call);            \
+    if (rc_ != 0) return rc_;    \
+  } while (0)
+
 void mmx_set_error(const char* msg);
 
 static inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }

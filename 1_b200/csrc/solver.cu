@@ -947,9 +947,44 @@ static int step_once(mmx_solver* s, cudaStream_t st) {
   return rk_step(s, st);
 }
 
+static bool rk_fixed(const mmx_solver* s) {
+  const bool bounds = s->p.min_dm != 0.f || s->p.max_dm != 0.f || s->p.min_dt != 0.f || s->p.max_dt != 0.f;
+  return s->p.solver != MMX_SOLVER_HEUN && !s->adaptive && !s->fsal && !bounds;
+}
+
+// One fixed-step RK step as pure launches (no host traffic), for graph
+// capture: the device dt and accept flag are uploaded beforehand.
+static cudaError_t rk_fixed_launches(mmx_solver* s, cudaStream_t st) {
+  float* dt_dev = s->scratch + 2;
+  const int* acc_dev = reinterpret_cast<const int*>(s->scratch + 3);
+  for (int i = 0; i < s->stages; i++) {
+    if (i == 0) {
+      cudaError_t e = cudaMemsetAsync(s->scratch + 1, 0, sizeof(float), st);
+      if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = rk_stage(s, i, st, dt_dev);
+    if (e != cudaSuccess) return e;
+  }
+  k_finalize_accept<<<solver_grid_1d(s->n), 256, 0, st>>>(s->m, s->mnew, s->n, acc_dev);
+  return cudaGetLastError();
+}
+
+static cudaError_t step_launches(mmx_solver* s, cudaStream_t st) {
+  return s->p.solver == MMX_SOLVER_HEUN ? heun_step(s, st) : rk_fixed_launches(s, st);
+}
+
 extern "C" int mmx_solver_step(mmx_solver* s, int nsteps, cudaStream_t st) {
   if (!s || nsteps < 0) { mmx_set_error("bad argument"); return MMX_ERR_ARG; }
-  bool graphable = s->use_graph && !s->profile && s->p.solver == MMX_SOLVER_HEUN && s->p.max_error == 0.f;
+  bool graphable = s->use_graph && !s->profile &&
+                   ((s->p.solver == MMX_SOLVER_HEUN && s->p.max_error == 0.f) || rk_fixed(s));
+  if (graphable && s->p.solver != MMX_SOLVER_HEUN && s->dt_uploaded != s->dt) {
+    float v[2] = {s->dt, 0.f};
+    int one = 1;
+    memcpy(&v[1], &one, sizeof(int));
+    MMX_TRY(cudaMemcpyAsync(s->scratch + 2, v, sizeof(v), cudaMemcpyHostToDevice, st));
+    MMX_TRY(cudaStreamSynchronize(st));
+    s->dt_uploaded = s->dt;
+  }
   for (int k = 0; k < nsteps; k++) {
     if (graphable) {
       if (!s->gexec || s->gstream != st) {
@@ -959,7 +994,7 @@ extern "C" int mmx_solver_step(mmx_solver* s, int nsteps, cudaStream_t st) {
         if (cap == 0) { MMX_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)); own = true; }
         cudaGraph_t g;
         MMX_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-        cudaError_t e = heun_step(s, cap);
+        cudaError_t e = step_launches(s, cap);
         cudaError_t e2 = cudaStreamEndCapture(cap, &g);
         if (own) cudaStreamDestroy(cap);
         if (e != cudaSuccess || e2 != cudaSuccess) { mmx_set_error("graph capture failed"); return MMX_ERR_CUDA; }

@@ -38,6 +38,7 @@ struct mmx_solver {
   float torque = 0, step_error = 0;
   long long steps = 0;
   int fsal_init = 0;
+  float dt_uploaded = -1.f;  // dt last written to the device scalar by the graph path
   // tableau
   int stages = 0, fsal = 0, adaptive = 0;
   double errorder = 1;

@@ -44,6 +44,12 @@ BATCH_WORKLOADS = {
     # BASELINE batching configuration: 256 instances, RK4, fixed dt 5e-15 s
     "batch-fp32-rk4-256": dict(count=256, seed=4, solver="rk4", dt=5e-15),
 }
+SERVE_WORKLOADS = {
+    # BASELINE serving configuration: Poisson 200 req/s, seed 5, relaxations
+    # (alpha 1, stop at max torque < 1e-4) and 21-point sweeps of B along x
+    # from -100 to +100 mT; a bounded sample of the stream's first requests.
+    "serve-fp32-rk4-mixed": dict(seed=5, rate=200.0, dt=1e-13, max_torque=1e-4, check_every=100, points=21),
+}
 DEFAULT = "plain-fp32-heun-256x256x32"
 
 
@@ -219,6 +225,91 @@ def run_batch(args, name):
     print(json.dumps(line), flush=True)
 
 
+def pct(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = min(len(xs) - 1, max(0, int(np.ceil(q / 100.0 * len(xs))) - 1))
+    return xs[k]
+
+
+def run_serve(args, name):
+    """The serving form: the request loop with continuous batching against
+    the same loop solving one request at a time (the plain form), on the
+    same requests with the same arrival times.  Requests of the stream are
+    partitioned over the ranks (no collective on the data path)."""
+    import torch
+    eng = importlib.import_module("1_b200")
+    sw = SERVE_WORKLOADS[name]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    reqs = eng.serve_stream(args.requests, seed=sw["seed"], rate=sw["rate"], dt=sw["dt"], sweep_points=sw["points"])
+    part = eng.partition_requests(reqs, world)
+    mine = [r for r, k in zip(reqs, part) if k == rank]
+    out = {}
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    arms = ["served", "plain"] if not args.no_plain else ["served"]
+    for arm in arms:
+        sv = eng.Server(batched=(arm == "served"), check_every=sw["check_every"], keep_m=True)
+        t0 = time.perf_counter()
+        res = eng.run_stream(sv, mine, realtime=True, max_torque=sw["max_torque"], max_steps=args.serve_max_steps)
+        wall = time.perf_counter() - t0
+        ms = {r["index"]: sv.result_m(r["id"]) for r in res}
+        st = sv.stats()
+        sv.close()
+        lat = [r["latency"] for r in res]
+        out[arm] = dict(res=res, m=ms, wall=wall, stats=st,
+                        solves_per_s=len(res) / wall if wall > 0 else 0.0,
+                        p50_ms=1e3 * pct(lat, 50), p99_ms=1e3 * pct(lat, 99),
+                        steps=sum(r["steps"] for r in res),
+                        converged=sum(1 for r in res if r["converged"]))
+    clk = clocks.stop()
+    same = None
+    if "plain" in out:
+        same = max(float(np.abs(out["served"]["m"][i] - out["plain"]["m"][i]).max()) for i in out["served"]["m"])
+    srv = out["served"]
+    cells = {r["index"]: int(np.prod(r["cfg"]["grid"])) for r in mine}
+    cell_steps = sum(cells[r["index"]] * r["steps"] for r in srv["res"])
+    line = {"metric": "solves/s", "value": srv["solves_per_s"], "unit": "solves/s", "n_gpus": world,
+            "steps": len(mine), "warmup": 0, "ms_per_step": 1e3 * srv["wall"] / max(1, len(mine)),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": name, "requests": len(mine), "stream_requests": len(reqs),
+                       "rate_per_s": sw["rate"], "seed": sw["seed"], "dt_s": sw["dt"],
+                       "max_torque": sw["max_torque"], "check_every": sw["check_every"],
+                       "sweep_points": sw["points"], "max_steps_per_point": args.serve_max_steps,
+                       "sample": "the first %d requests of the stream, arriving in real time" % len(reqs)},
+            "latency_ms": {"p50": srv["p50_ms"], "p99": srv["p99_ms"]},
+            "served": {"solves_per_s": srv["solves_per_s"], "wall_s": srv["wall"], "steps": srv["steps"],
+                       "cell_steps_per_s": cell_steps / srv["wall"], "converged": srv["converged"],
+                       "chunks": srv["stats"]["chunks"], "regroups": srv["stats"]["regroups"]},
+            "clocks": clk}
+    if "plain" in out:
+        pl = out["plain"]
+        line["plain"] = {"solves_per_s": pl["solves_per_s"], "wall_s": pl["wall"], "p50_ms": pl["p50_ms"],
+                         "p99_ms": pl["p99_ms"], "steps": pl["steps"]}
+        line["speedup_vs_plain"] = srv["solves_per_s"] / pl["solves_per_s"] if pl["solves_per_s"] else None
+        line["served_vs_plain_max_abs_dm"] = same
+    line["per_request"] = [{"i": r["index"], "kind": r["kind"], "grid": list(next(q["cfg"]["grid"] for q in mine
+                                                                               if q["index"] == r["index"])),
+                            "steps": r["steps"], "latency_ms": 1e3 * r["latency"], "converged": r["converged"]}
+                           for r in srv["res"]]
+    if world > 1:
+        import torch.distributed as dist
+        lines = [None] * world
+        dist.gather_object(line, lines if rank == 0 else None, dst=0)
+        if rank == 0:
+            tot = sum(len(l["per_request"]) for l in lines)
+            wall = max(l["served"]["wall_s"] for l in lines)
+            lat = [q["latency_ms"] for l in lines for q in l["per_request"]]
+            line["value"] = tot / wall
+            line["latency_ms"] = {"p50": pct(lat, 50), "p99": pct(lat, 99)}
+            line["config"]["requests"] = tot
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_reference(args, w, name):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -361,9 +452,19 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT,
+                    choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) + sorted(SERVE_WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--requests", type=int, default=16, help="serving: requests of the stream to run")
+    ap.add_argument("--serve-max-steps", type=int, default=0, help="serving: step cap per relaxation (0: none)")
+    ap.add_argument("--no-plain", action="store_true", help="serving: skip the one-at-a-time arm")
     args = ap.parse_args()
+    if args.workload in SERVE_WORKLOADS:
+        if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+            import torch.distributed as dist
+            dist.init_process_group("gloo", init_method="env://")
+        run_serve(args, args.workload)
+        return
     if args.workload in BATCH_WORKLOADS:
         run_batch(args, args.workload)
         return

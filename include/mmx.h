@@ -136,6 +136,63 @@ mmx_solver* mmx_batch_instance(mmx_batch* b, int i);
 int mmx_batch_size(mmx_batch* b, int* count, long long* cells, int* launches_per_step);
 int mmx_batch_step(mmx_batch* b, int nsteps, cudaStream_t stream);
 int mmx_batch_use_graph(mmx_batch* b, int on);
+/* The maximum torque of every instance in the last RK4 step, gathered into
+ * out (count floats; host when on_host != 0, asynchronous on 'stream'). */
+int mmx_batch_torques(mmx_batch* b, float* out, int on_host, cudaStream_t stream);
+
+/* Serving form: a request loop with continuous batching.  A request is a
+ * relaxation (npoints == 1, Sim.Relax, src/go/sim/relax.go:14-23) or a field
+ * sweep (npoints > 1 fields, a relaxation at each, Sim.Hysteresis,
+ * simhysteresis.go:16-27) of one solve with the fixed-step RK4 solver.  A
+ * relaxation stops when the maximum torque max|k0| of a step (the
+ * reference's 'torque', rk.go:353-354, internal units) is below max_torque;
+ * it is checked every check_every steps of that solve.  Admission is FIFO,
+ * bounded by the device bytes of the resident solves (mmx_server_footprint)
+ * and by max_active.  Each mmx_server_pump advances every resident solve by
+ * check_every steps -- in one mmx_batch when 'batched', else one solve at a
+ * time on the single-instance solver (the baseline) -- then retires the
+ * solves that finished and admits queued ones into the freed room.  A
+ * request's result does not depend on the other resident solves. */
+#define MMX_REQ_QUEUED 0
+#define MMX_REQ_ACTIVE 1
+#define MMX_REQ_DONE 2
+#define MMX_REQ_FAILED 3
+typedef struct mmx_request {
+  mmx_params params;         /* solver must be MMX_SOLVER_RK4 with max_error 0 */
+  const float* m0;           /* initial m, host [3][X][Y][Z]; copied by submit */
+  int npoints;               /* 1: relax under params.hext; > 1: sweep */
+  const float* hext_points;  /* npoints x 3 internal fields, or NULL when npoints == 1 */
+  float max_torque;          /* relaxation stop threshold (> 0) */
+  long long max_steps;       /* cap per relaxation (0: none); a capped point is not 'converged' */
+} mmx_request;
+typedef struct mmx_server_config {
+  size_t hbm_budget;         /* device bytes the resident solves may hold (0: 80% of free) */
+  int max_active;            /* resident solves at most (0: no limit) */
+  int check_every;           /* steps per pump: the stop-check interval */
+  int batched;               /* 1: continuous batching; 0: one solve at a time */
+  int keep_m;                /* keep each finished solve's final m on the host */
+} mmx_server_config;
+typedef struct mmx_result {
+  int state;                 /* MMX_REQ_* */
+  int converged;             /* every point met max_torque */
+  long long steps;           /* steps taken over all points */
+  int points_done;
+  double t_submit, t_admit, t_done;  /* seconds on the server clock (-1: not yet) */
+  size_t footprint;          /* device bytes the solve held while resident */
+} mmx_result;
+typedef struct mmx_server mmx_server;
+int mmx_server_create(const mmx_server_config* cfg, cudaStream_t stream, mmx_server** out);
+int mmx_server_destroy(mmx_server* sv);
+int mmx_server_footprint(const mmx_params* p, size_t* bytes);
+int mmx_server_submit(mmx_server* sv, const mmx_request* r, long long* id);
+int mmx_server_pump(mmx_server* sv, int* n_active, int* n_queued);
+/* avg_m: 3 floats per finished point (<m> after its relaxation);
+ * point_steps: steps per finished point.  Either may be NULL. */
+int mmx_server_result(mmx_server* sv, long long id, mmx_result* out, float* avg_m, long long* point_steps);
+int mmx_server_result_m(mmx_server* sv, long long id, float* m_host);
+int mmx_server_release(mmx_server* sv, long long id);
+double mmx_server_clock(mmx_server* sv);
+int mmx_server_stats(mmx_server* sv, size_t* used_bytes, long long* chunks, long long* regroups);
 
 /* Allocation-free reduction.  No counterpart in the reference: a variant of
  * gpu_reduce (same operations, 1 add, 2 max, 3 max |x|, 4 min, 5 sum |x|)

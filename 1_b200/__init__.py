@@ -20,7 +20,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-LIB_PATH = os.path.join(HERE, "libgpukern.so")
+# MMX_LIBGPUKERN selects another build of the library (e.g. one compiled with
+# different tile shapes); the default is the in-tree build.
+LIB_PATH = os.environ.get("MMX_LIBGPUKERN", os.path.join(HERE, "libgpukern.so"))
 DRIVER_PATH = os.path.join(HERE, "libmmxdriver.so")
 
 SOLVERS = {"heun": 0, "rk12": 1, "rk23": 2, "rk4": 3, "rkck": 4, "rkdp": 5, "rk2": 6}
@@ -234,6 +236,7 @@ MMX = {
     "mmx_batch_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "mmx_batch_use_graph": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "mmx_batch_create_from": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "mmx_batch_tuning": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     "mmx_batch_torques": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     "mmx_solver_torque_device": (ctypes.c_void_p, [ctypes.c_void_p]),
     "mmx_server_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
@@ -490,6 +493,20 @@ class Batch:
         _check(lib().mmx_batch_use_graph(self.h, 1 if on else 0))
 
 
+def batch_tuning():
+    """The autotuner's decisions for the batched Y passes: one dict per
+    (line length, direction) with both tile widths, their measured launch
+    times (ms) and the width kept."""
+    n = ctypes.c_int()
+    _check(lib().mmx_batch_tuning(0, None, None, ctypes.byref(n)))
+    rows = np.zeros((max(n.value, 1), 5), np.int32)
+    ms = np.zeros((max(n.value, 1), 2), np.float32)
+    _check(lib().mmx_batch_tuning(n.value, rows.ctypes.data, ms.ctypes.data, ctypes.byref(n)))
+    return [dict(L=int(r[0]), inverse=bool(r[1]), widths=(int(r[2]), int(r[3])), ms=(float(m[0]), float(m[1])),
+                 chosen=int(r[3] if r[4] else r[2]))
+            for r, m in zip(rows[:n.value], ms[:n.value])]
+
+
 def batch_config(count, seed=4, cell=3e-9, solver="rk4", dt=5e-15):
     """The batch configuration: count instances with Nx, Ny drawn from
     {32,48,64,96,128,192,256}, Nz from {1,2,4}, Ms ~ U[4e5,1.4e6] A/m,
@@ -626,13 +643,30 @@ def sweep_fields(msat, aexch, b0, b1, points):
     return out
 
 
-def serve_stream(count, seed=5, rate=200.0, cell=3e-9, dt=1e-13, sweep_points=21, sweep_fraction=0.5,
+def stable_dt(grid, cell, msat, aexch, alpha, bmag=0.0, safety=2.0):
+    """A fixed RK4 time step (s) inside the stability region of the
+    linearised LLG operator: the six-neighbour exchange Laplacian's largest
+    eigenvalue sum_d 4/c_d^2 (internal cell sizes, axes with more than one
+    cell), plus 1 for the demagnetising field and |B| in internal units; the
+    LLG eigenvalues have modulus lambda/sqrt(1+alpha^2), and RK4 is stable
+    up to about 2.8 along the directions they take, so dt = safety *
+    sqrt(1+alpha^2) / lambda internal time units."""
+    u = units(msat, aexch)
+    L = float(u["length"])
+    lam = sum(4.0 / (c / L) ** 2 for c, n in zip(cell, grid) if n > 1)
+    lam += 1.0 + bmag / float(u["field"])
+    return safety * float(np.sqrt(1.0 + alpha * alpha)) / lam * float(u["time"])
+
+
+def serve_stream(count, seed=5, rate=200.0, cell=3e-9, dt=None, sweep_points=21, sweep_fraction=0.5,
                  bmax=0.1):
     """The serving workload: a Poisson stream (rate requests/s) of
     relaxations (alpha = 1, under a uniform field drawn as in the batch
     configuration) and field sweeps (alpha = 1, B along user x from -bmax to
     +bmax tesla in sweep_points points), sizes and materials drawn as in
-    batch_config, random unit m per cell.  Per request, in order: the
+    batch_config, random unit m per cell.  dt: a fixed step in seconds, or
+    None for each request's stable_dt (the relaxation is a steady state, so
+    the step only sets how many steps it takes).  Per request, in order: the
     inter-arrival gap, the kind, then the batch_config draws; m comes from
     its own generator seeded (seed, index).  Returns dicts with 'arrival'
     (s), 'kind', 'cfg' (user-level) and 'fields' (None or internal)."""
@@ -652,8 +686,10 @@ def serve_stream(count, seed=5, rate=200.0, cell=3e-9, dt=1e-13, sweep_points=21
         d = rng.standard_normal(3)
         d = d / np.linalg.norm(d)
         bmag = float(rng.uniform(0.0, bmax))
+        step = dt if dt is not None else stable_dt((nx, ny, nz), (cell, cell, cell), ms, a, 1.0,
+                                                   bmax if sweep else bmag)
         cfg = dict(grid=(nx, ny, nz), cell=(cell, cell, cell), msat=ms, aexch=a, alpha=1.0,
-                   bext=(0.0, 0.0, 0.0) if sweep else tuple(float(x) for x in bmag * d), solver="rk4", dt=dt)
+                   bext=(0.0, 0.0, 0.0) if sweep else tuple(float(x) for x in bmag * d), solver="rk4", dt=step)
         fields = sweep_fields(ms, a, (-bmax, 0.0, 0.0), (bmax, 0.0, 0.0), sweep_points) if sweep else None
         if sweep:
             cfg["bext"] = (-bmax, 0.0, 0.0)

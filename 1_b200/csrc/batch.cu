@@ -11,6 +11,7 @@
 // {1,2,4}) a Runge-Kutta stage is at most ~35 launches whatever the number
 // of instances, and a whole step is captured in one CUDA graph.
 #include <map>
+#include <mutex>
 #include <string.h>
 #include <vector>
 
@@ -93,6 +94,8 @@ struct Launch {
   int blocks;
   void* args;     // device array of per-instance argument structs
   int* starts;    // device array of tile offsets
+  int variant = 0;  // tile shape (column passes: 0 = fx_col_tk, 1 = col_tk_alt)
+  size_t args_off = 0, starts_off = 0;  // offsets into the batch's table block
 };
 enum { L_ZR2C = 0, L_COL = 1, L_CONV = 2, L_ZINV = 3, L_FIN = 4 };
 
@@ -110,7 +113,31 @@ struct mmx_batch {
   int launches_per_step = 0;
   float** torque_ptrs = nullptr;  // RK4: per-instance max |k0| slots, cleared each step
   float* gather = nullptr;        // device staging of the gathered torques
+  // graph capture: the launches of one pass (one per line length) are
+  // independent and run as parallel branches
+  std::vector<cudaStream_t> par;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
+  // every launch's argument and tile-offset tables live in one device block,
+  // staged on the host while the launches are built
+  std::vector<char> blob;
+  char* dblob = nullptr;
+  // per instance: offsets in the block of its Zeeman field in every
+  // epilogue table, so a field can change without rebuilding the batch
+  std::vector<std::vector<size_t>> hext_off;
 };
+
+// pass of a launch within a field evaluation; launches of the same pass
+// touch disjoint instances
+static int phase_of(const Launch& l) {
+  switch (l.kind) {
+    case L_ZR2C: return 0;
+    case L_COL: return l.flag ? 3 : 1;
+    case L_CONV: return 2;
+    case L_ZINV: return 4;
+    default: return 5;
+  }
+}
 
 __global__ void kb_clear(float** p, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -125,9 +152,14 @@ static void set_smem(K kern, size_t bytes) {
   if (bytes > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-template <int L>
-static cudaError_t run_col(const Launch& l, cudaStream_t st) {
-  constexpr int TK = fx_col_tk(L);
+// The autotuner's alternative column-tile width: half the default where
+// that leaves >= 8 columns (more, smaller blocks), else double (fewer,
+// larger blocks).
+__host__ __device__ constexpr int col_tk_alt(int L) { return fx_col_tk(L) >= 16 ? fx_col_tk(L) / 2 : 2 * fx_col_tk(L); }
+__host__ __device__ constexpr int col_tk_variant(int L, int v) { return v ? col_tk_alt(L) : fx_col_tk(L); }
+
+template <int L, int TK>
+static cudaError_t run_col_tk(const Launch& l, cudaStream_t st) {
   constexpr int T = fx_threads(TK * L);
   size_t smem = sizeof(float2) * (size_t)odd_pitch(TK) * L;
   if (l.flag) {
@@ -138,6 +170,10 @@ static cudaError_t run_col(const Launch& l, cudaStream_t st) {
     kb_col<L, TK, T, false><<<l.blocks, T, smem, st>>>((const BCol*)l.args, l.starts, l.nseg);
   }
   return cudaGetLastError();
+}
+template <int L>
+static cudaError_t run_col(const Launch& l, cudaStream_t st) {
+  return l.variant ? run_col_tk<L, col_tk_alt(L)>(l, st) : run_col_tk<L, fx_col_tk(L)>(l, st);
 }
 template <int L>
 static int conv_tk() {
@@ -237,9 +273,61 @@ static cudaError_t run_launch(const Launch& l, cudaStream_t st) {
 // ---------------------------------------------------------------------
 // building the launch tables
 // ---------------------------------------------------------------------
+// Appends a launch whose tables are staged in the batch's host block; the
+// device pointers are set by batch_upload once every launch is built.
+static size_t blob_put(mmx_batch* b, const void* data, size_t bytes) {
+  size_t off = (b->blob.size() + 255) & ~(size_t)255;
+  b->blob.resize(off + bytes);
+  memcpy(b->blob.data() + off, data, bytes);
+  return off;
+}
 template <typename A>
 static int add_launch(mmx_batch* b, std::vector<Launch>& out, int kind, int L, int flag, const std::vector<A>& args,
                       const std::vector<int>& tiles) {
+  if (args.empty()) return MMX_OK;
+  Launch l;
+  l.kind = kind;
+  l.L = L;
+  l.flag = flag;
+  l.nseg = (int)args.size();
+  std::vector<int> starts(args.size());
+  int acc = 0;
+  for (size_t i = 0; i < args.size(); i++) {
+    starts[i] = acc;
+    acc += tiles[i];
+  }
+  l.blocks = acc;
+  l.args = nullptr;
+  l.starts = nullptr;
+  l.args_off = blob_put(b, args.data(), sizeof(A) * args.size());
+  l.starts_off = blob_put(b, starts.data(), sizeof(int) * starts.size());
+  out.push_back(l);
+  return MMX_OK;
+}
+static int batch_upload(mmx_batch* b) {
+  if (b->blob.empty()) return MMX_OK;
+  if (cudaMalloc(&b->dblob, b->blob.size()) != cudaSuccess) {
+    mmx_set_error("out of device memory (batch tables)");
+    return MMX_ERR_MEM;
+  }
+  b->owned.push_back(b->dblob);
+  MMX_TRY(cudaMemcpy(b->dblob, b->blob.data(), b->blob.size(), cudaMemcpyHostToDevice));
+  auto patch = [&](std::vector<Launch>& ls) {
+    for (Launch& l : ls) {
+      l.args = b->dblob + l.args_off;
+      l.starts = reinterpret_cast<int*>(b->dblob + l.starts_off);
+    }
+  };
+  for (auto& st : b->stage) patch(st);
+  patch(b->finalize);
+  return MMX_OK;
+}
+
+// A launch with its own device tables, usable at once (the autotuner's
+// timing runs).
+template <typename A>
+static int add_launch_now(mmx_batch* b, std::vector<Launch>& out, int kind, int L, int flag, const std::vector<A>& args,
+                          const std::vector<int>& tiles) {
   if (args.empty()) return MMX_OK;
   Launch l;
   l.kind = kind;
@@ -266,11 +354,11 @@ static int add_launch(mmx_batch* b, std::vector<Launch>& out, int kind, int L, i
   return MMX_OK;
 }
 
-static int col_tiles(int L, int ncols, int nplanes) {
+static int col_tiles(int L, int ncols, int nplanes, int variant) {
   int tk = 1;
   switch (L) {
 #define C_(LL) \
-  case LL: tk = fx_col_tk(LL); break;
+  case LL: tk = col_tk_variant(LL, variant); break;
     FX_SIZES(C_)
 #undef C_
   }
@@ -294,6 +382,127 @@ static int zrows_per_tile(int M, int lines_per_row) {
 #undef C_
   }
   return 1;
+}
+
+// ---------------------------------------------------------------------
+// Autotuner of the column (Y) passes.  For each line length and direction
+// the first batch that needs it times both compiled tile widths
+// (col_tk_variant) on its own instances -- the Y passes read and write only
+// the spectrum buffers, which hold no state between field evaluations, so
+// timing them changes nothing -- and keeps the faster.  The choice is kept
+// for the process (every later batch, e.g. each regrouping of a serving
+// loop, reuses it).  Either width computes every line with the same
+// arithmetic, so the choice never changes a result.
+// ---------------------------------------------------------------------
+struct ColTune {
+  int L, inv, tk0, tk1, chosen;
+  float ms0, ms1;
+};
+static std::map<std::pair<int, int>, ColTune> g_col_tune;
+static std::mutex g_col_tune_mu;
+
+static void col_args(mmx_batch* b, int L, int inv, const std::vector<int>& ids, int variant, std::vector<BCol>& a,
+                     std::vector<int>& t) {
+  a.clear();
+  t.clear();
+  for (int i : ids) {
+    mmx_solver* s = b->inst[i];
+    BCol c;
+    c.src = s->S;
+    c.dst = s->S;
+    c.cp.f = s->bp.fy;
+    c.cp.nplanes = 3 * s->N[0];
+    c.cp.plane_stride = (int64_t)s->P[1] * s->HZ;
+    c.cp.ncols = s->HZ;
+    c.cp.stride_i = s->HZ;
+    c.cp.n_in = inv ? s->P[1] : s->N[1];
+    c.cp.n_out = inv ? s->N[1] : s->P[1];
+    c.cp.inv = inv;
+    int tiles = col_tiles(L, c.cp.ncols, c.cp.nplanes, variant);
+    c.ntx = tiles / c.cp.nplanes;
+    a.push_back(c);
+    t.push_back(tiles);
+  }
+}
+
+static float time_launch(const Launch& l, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1) {
+  if (run_launch(l, st) != cudaSuccess) return -1.f;  // warm-up
+  cudaEventRecord(e0, st);
+  for (int r = 0; r < 3; r++) run_launch(l, st);
+  cudaEventRecord(e1, st);
+  if (cudaEventSynchronize(e1) != cudaSuccess) return -1.f;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  return ms / 3.f;
+}
+
+static int add_col_launch(mmx_batch* b, std::vector<Launch>& out, int L, int inv, const std::vector<int>& ids) {
+  std::vector<BCol> a;
+  std::vector<int> t;
+  int rc;
+  std::lock_guard<std::mutex> lock(g_col_tune_mu);
+  auto key = std::make_pair(L, inv);
+  auto it = g_col_tune.find(key);
+  int variant = 0;
+  if (it != g_col_tune.end()) {
+    variant = it->second.chosen;
+  } else {
+    ColTune ct;
+    ct.L = L;
+    ct.inv = inv;
+    ct.tk0 = ct.tk1 = 0;
+    switch (L) {
+#define C_(LL) \
+  case LL: ct.tk0 = col_tk_variant(LL, 0); ct.tk1 = col_tk_variant(LL, 1); break;
+      FX_SIZES(C_)
+#undef C_
+    }
+    float ms[2] = {-1.f, -1.f};
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess &&
+        cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
+      for (int v = 0; v < 2; v++) {
+        std::vector<Launch> tmp;
+        col_args(b, L, inv, ids, v, a, t);
+        if ((rc = add_launch_now(b, tmp, L_COL, L, inv, a, t)) != MMX_OK) break;
+        tmp.back().variant = v;
+        ms[v] = time_launch(tmp.back(), st, e0, e1);
+      }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (st) cudaStreamDestroy(st);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { mmx_set_error(cudaGetErrorString(e)); return MMX_ERR_CUDA; }
+    ct.ms0 = ms[0];
+    ct.ms1 = ms[1];
+    ct.chosen = (ms[1] > 0.f && ms[0] > 0.f && ms[1] < ms[0]) ? 1 : 0;
+    g_col_tune[key] = ct;
+    variant = ct.chosen;
+  }
+  col_args(b, L, inv, ids, variant, a, t);
+  if ((rc = add_launch(b, out, L_COL, L, inv, a, t)) != MMX_OK) return rc;
+  out.back().variant = variant;
+  return MMX_OK;
+}
+
+extern "C" int mmx_batch_tuning(int max, int* rows, float* ms, int* n) {
+  if (!n || (max > 0 && (!rows || !ms))) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  std::lock_guard<std::mutex> lock(g_col_tune_mu);
+  int k = 0;
+  for (auto& kv : g_col_tune) {
+    if (k < max) {
+      const ColTune& c = kv.second;
+      int* r = rows + 5 * k;
+      r[0] = c.L; r[1] = c.inv; r[2] = c.tk0; r[3] = c.tk1; r[4] = c.chosen;
+      ms[2 * k] = c.ms0;
+      ms[2 * k + 1] = c.ms1;
+    }
+    k++;
+  }
+  *n = k;
+  return MMX_OK;
 }
 
 // Builds the launches of one field evaluation: zfwd (optionally with the
@@ -332,29 +541,8 @@ static int build_eval(mmx_batch* b, std::vector<Launch>& out, int mode, bool com
     if ((rc = add_launch(b, out, L_ZR2C, g.first, comb ? 1 : 0, a, t)) != MMX_OK) return rc;
   }
   // Y forward (3D)
-  for (auto& g : byP1_3d) {
-    std::vector<BCol> a;
-    std::vector<int> t;
-    for (int i : g.second) {
-      mmx_solver* s = b->inst[i];
-      BCol c;
-      c.src = s->S;
-      c.dst = s->S;
-      c.cp.f = s->bp.fy;
-      c.cp.nplanes = 3 * s->N[0];
-      c.cp.plane_stride = (int64_t)s->P[1] * s->HZ;
-      c.cp.ncols = s->HZ;
-      c.cp.stride_i = s->HZ;
-      c.cp.n_in = s->N[1];
-      c.cp.n_out = s->P[1];
-      c.cp.inv = 0;
-      int tiles = col_tiles(g.first, c.cp.ncols, c.cp.nplanes);
-      c.ntx = tiles / c.cp.nplanes;
-      a.push_back(c);
-      t.push_back(tiles);
-    }
-    if ((rc = add_launch(b, out, L_COL, g.first, 0, a, t)) != MMX_OK) return rc;
-  }
+  for (auto& g : byP1_3d)
+    if ((rc = add_col_launch(b, out, g.first, 0, g.second)) != MMX_OK) return rc;
   // X convolution (3D) and Y convolution (2D)
   for (int d2 = 0; d2 < 2; d2++) {
     auto& groups = d2 ? byP1_2d : byP0;
@@ -388,29 +576,8 @@ static int build_eval(mmx_batch* b, std::vector<Launch>& out, int mode, bool com
     }
   }
   // Y inverse (3D)
-  for (auto& g : byP1_3d) {
-    std::vector<BCol> a;
-    std::vector<int> t;
-    for (int i : g.second) {
-      mmx_solver* s = b->inst[i];
-      BCol c;
-      c.src = s->S;
-      c.dst = s->S;
-      c.cp.f = s->bp.fy;
-      c.cp.nplanes = 3 * s->N[0];
-      c.cp.plane_stride = (int64_t)s->P[1] * s->HZ;
-      c.cp.ncols = s->HZ;
-      c.cp.stride_i = s->HZ;
-      c.cp.n_in = s->P[1];
-      c.cp.n_out = s->N[1];
-      c.cp.inv = 1;
-      int tiles = col_tiles(g.first, c.cp.ncols, c.cp.nplanes);
-      c.ntx = tiles / c.cp.nplanes;
-      a.push_back(c);
-      t.push_back(tiles);
-    }
-    if ((rc = add_launch(b, out, L_COL, g.first, 1, a, t)) != MMX_OK) return rc;
-  }
+  for (auto& g : byP1_3d)
+    if ((rc = add_col_launch(b, out, g.first, 1, g.second)) != MMX_OK) return rc;
   // Z inverse + epilogue
   for (auto& g : byM) {
     std::vector<ZinvArgs> a;
@@ -430,6 +597,9 @@ static int build_eval(mmx_batch* b, std::vector<Launch>& out, int mode, bool com
       t.push_back(div_up(z.nrows, zrows_per_tile(g.first, 3)));
     }
     if ((rc = add_launch(b, out, L_ZINV, g.first, mode, a, t)) != MMX_OK) return rc;
+    for (size_t k = 0; k < g.second.size(); k++)
+      b->hext_off[g.second[k]].push_back(out.back().args_off + k * sizeof(ZinvArgs) + offsetof(ZinvArgs, ea) +
+                                         offsetof(EpiArgs, lf) + offsetof(LocalField, hext));
   }
   return MMX_OK;
 }
@@ -437,6 +607,9 @@ static int build_eval(mmx_batch* b, std::vector<Launch>& out, int mode, bool com
 static void batch_free(mmx_batch* b) {
   if (!b) return;
   if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  for (cudaStream_t q : b->par) cudaStreamDestroy(q);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  for (cudaEvent_t e : b->ev_join) cudaEventDestroy(e);
   for (void* p : b->owned) cudaFree(p);
   if (b->owns)
     for (mmx_solver* s : b->inst) mmx_solver_destroy(s);
@@ -459,6 +632,7 @@ static int batch_check(mmx_solver* s, int solver) {
 
 static int batch_build(mmx_batch* b) {
   int rc = MMX_OK;
+  b->hext_off.assign(b->inst.size(), std::vector<size_t>());
   for (mmx_solver* s : b->inst) {
     // the stage kernels read dt from the instance's device scalar
     MMX_TRY(cudaMemcpy(s->scratch + 2, &s->dt, sizeof(float), cudaMemcpyHostToDevice));
@@ -552,6 +726,7 @@ static int batch_build(mmx_batch* b) {
     }
   }
   if (rc != MMX_OK) return rc;
+  if ((rc = batch_upload(b)) != MMX_OK) return rc;
   for (auto& st : b->stage) b->launches_per_step += (int)st.size();
   b->launches_per_step += (int)b->finalize.size() + (b->torque_ptrs ? 1 : 0);
   return MMX_OK;
@@ -613,18 +788,52 @@ extern "C" mmx_solver* mmx_batch_instance(mmx_batch* b, int i) {
   return b->inst[i];
 }
 
-static cudaError_t batch_step_launches(mmx_batch* b, cudaStream_t st) {
+#define BATCH_MAX_PAR 8
+
+// Launches ls[0..n) of one pass on parallel branches forked from st and
+// joined back into it (used while st is being captured into a graph).
+static cudaError_t run_pass_parallel(mmx_batch* b, const Launch* ls, int n, cudaStream_t st) {
+  if (n == 1) return run_launch(ls[0], st);
+  cudaError_t e;
+  while ((int)b->par.size() < BATCH_MAX_PAR) {
+    cudaStream_t q;
+    if ((e = cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    b->par.push_back(q);
+    cudaEvent_t ev;
+    if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+    b->ev_join.push_back(ev);
+  }
+  if (!b->ev_fork && (e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming)) != cudaSuccess) return e;
+  const int P = n < BATCH_MAX_PAR ? n : BATCH_MAX_PAR;
+  if ((e = cudaEventRecord(b->ev_fork, st)) != cudaSuccess) return e;
+  for (int k = 0; k < P; k++)
+    if ((e = cudaStreamWaitEvent(b->par[k], b->ev_fork, 0)) != cudaSuccess) return e;
+  for (int i = 0; i < n; i++)
+    if ((e = run_launch(ls[i], b->par[i % P])) != cudaSuccess) return e;
+  for (int k = 0; k < P; k++) {
+    if ((e = cudaEventRecord(b->ev_join[k], b->par[k])) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(st, b->ev_join[k], 0)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+static cudaError_t batch_step_launches(mmx_batch* b, cudaStream_t st, bool parallel) {
   if (b->torque_ptrs) {
     int n = (int)b->inst.size();
     kb_clear<<<(n + 255) / 256, 256, 0, st>>>(b->torque_ptrs, n);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  for (auto& stage : b->stage)
-    for (const Launch& l : stage) {
-      cudaError_t e = run_launch(l, st);
+  for (auto& stage : b->stage) {
+    for (size_t i = 0; i < stage.size();) {
+      size_t j = i + 1;
+      if (parallel)
+        while (j < stage.size() && phase_of(stage[j]) == phase_of(stage[i])) j++;
+      cudaError_t e = run_pass_parallel(b, &stage[i], (int)(j - i), st);
       if (e != cudaSuccess) return e;
+      i = j;
     }
+  }
   for (const Launch& l : b->finalize) {
     cudaError_t e = run_launch(l, st);
     if (e != cudaSuccess) return e;
@@ -643,7 +852,7 @@ extern "C" int mmx_batch_step(mmx_batch* b, int nsteps, cudaStream_t st) {
         if (cap == 0) { MMX_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)); own = true; }
         cudaGraph_t g;
         MMX_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-        cudaError_t e = batch_step_launches(b, cap);
+        cudaError_t e = batch_step_launches(b, cap, true);
         cudaError_t e2 = cudaStreamEndCapture(cap, &g);
         if (own) cudaStreamDestroy(cap);
         if (e != cudaSuccess || e2 != cudaSuccess) { mmx_set_error("batch graph capture failed"); return MMX_ERR_CUDA; }
@@ -653,7 +862,7 @@ extern "C" int mmx_batch_step(mmx_batch* b, int nsteps, cudaStream_t st) {
       }
       MMX_TRY(cudaGraphLaunch(b->gexec, st));
     } else {
-      cudaError_t e = batch_step_launches(b, st);
+      cudaError_t e = batch_step_launches(b, st, false);
       if (e != cudaSuccess) { mmx_set_error(cudaGetErrorString(e)); return MMX_ERR_CUDA; }
     }
     for (mmx_solver* s : b->inst) {
@@ -681,6 +890,16 @@ extern "C" int mmx_batch_torques(mmx_batch* b, float* out, int on_host, cudaStre
   kb_gather<<<(n + 255) / 256, 256, 0, st>>>(b->torque_ptrs, n, dst);
   MMX_TRY(cudaGetLastError());
   if (on_host) MMX_TRY(cudaMemcpyAsync(out, b->gather, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+  return MMX_OK;
+}
+
+extern "C" int mmx_batch_set_hext(mmx_batch* b, int i, const float hext[3]) {
+  if (!b || !hext || i < 0 || i >= (int)b->inst.size()) { mmx_set_error("bad argument"); return MMX_ERR_ARG; }
+  MMX_CHECK_RC(mmx_solver_set_hext(b->inst[i], hext));
+  for (size_t off : b->hext_off[i]) {
+    memcpy(b->blob.data() + off, hext, 3 * sizeof(float));
+    MMX_TRY(cudaMemcpy(b->dblob + off, hext, 3 * sizeof(float), cudaMemcpyHostToDevice));
+  }
   return MMX_OK;
 }
 

@@ -28,9 +28,10 @@ struct LineFFT {
   int tws;                     // table stride (table built for a multiple of L)
 };
 
+// complex product with two fused multiply-adds (the transforms are
+// compared with the FP64 oracle within a tolerance, never bit for bit)
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)),
-                     __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -83,6 +84,30 @@ __device__ __forceinline__ void Radix<8>::dft(float2* v, bool inv) {
   v[6] = csub(e[2], o2);
   v[3] = cadd(e[3], o3);
   v[7] = csub(e[3], o3);
+}
+
+// Radix 16 (fixed-size transforms only): two radix-8 DFTs of the even and
+// odd samples combined with the twiddles W16^k.
+template <>
+__device__ __forceinline__ void Radix<16>::dft(float2* v, bool inv) {
+  float2 e[8], o[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    e[k] = v[2 * k];
+    o[k] = v[2 * k + 1];
+  }
+  Radix<8>::dft(e, inv);
+  Radix<8>::dft(o, inv);
+  const float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f, h = 0.70710678118654752440f;
+  // W16^k = exp(-+ 2 pi i k / 16), k = 1..7 (conjugated for the inverse)
+  const float wr[8] = {1.f, c1, h, s1, 0.f, -s1, -h, -c1};
+  const float wi[8] = {0.f, s1, h, c1, 1.f, c1, h, s1};
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    float2 t = k == 0 ? o[0] : k == 4 ? mul_mi(o[4], inv) : cmul(o[k], make_float2(wr[k], inv ? wi[k] : -wi[k]));
+    v[k] = cadd(e[k], t);
+    v[k + 8] = csub(e[k], t);
+  }
 }
 
 // Odd radices: direct DFT with constant twiddles cos/sin(2 pi k / R).

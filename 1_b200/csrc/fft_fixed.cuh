@@ -9,8 +9,8 @@
 // store straight to global memory (pruned outputs are not stored), so a
 // transform of R^s points makes s-1 round trips through shared memory.
 //
-// Radix plan: radix-8 stages first, then 4 or 2, then 3, 5, 7 (a line
-// length is any product of these); the inverse applies the stages in
+// Radix plan: radix-16 or radix-8 stages first, then 4 or 2, then 3, 5, 7
+// (a line length is any product of these); the inverse applies the stages in
 // reverse order, so that the last forward stage and the first inverse stage
 // group the same elements in the same thread (the kernel multiplication
 // between them stays in registers).
@@ -29,8 +29,15 @@ __device__ __forceinline__ float2 cmulc_f(float2 a, float2 b) {  // a * conj(b)
 __host__ __device__ constexpr int ilog2c(int x) { return x <= 1 ? 0 : 1 + ilog2c(x >> 1); }
 // Radix plan of a line length L = 2^a 3^b 5^c 7^d: radix 8 while 8 divides
 // the rest, then 4 or 2, then the odd radices.
-__host__ __device__ constexpr int first_radix(int L) {
+__host__ __device__ constexpr int first_radix8(int L) {
   return L % 8 == 0 ? 8 : L % 4 == 0 ? 4 : L % 2 == 0 ? 2 : L % 3 == 0 ? 3 : L % 5 == 0 ? 5 : 7;
+}
+__host__ __device__ constexpr int n_stages8(int L) { return L <= 1 ? 0 : 1 + n_stages8(L / first_radix8(L)); }
+// Radix 16 first when it saves a stage (one shared-memory round trip),
+// e.g. 256 = 16*16 instead of 8*8*4.
+__host__ __device__ constexpr int n_stages(int L);
+__host__ __device__ constexpr int first_radix(int L) {
+  return (L % 16 == 0 && 1 + n_stages(L / 16) < n_stages8(L)) ? 16 : first_radix8(L);
 }
 __host__ __device__ constexpr int n_stages(int L) { return L <= 1 ? 0 : 1 + n_stages(L / first_radix(L)); }
 // radix of forward stage st

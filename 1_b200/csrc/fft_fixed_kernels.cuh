@@ -206,10 +206,10 @@ __device__ __forceinline__ void conv_body(const ConvArgs& a, int bx) {
       float Kxx, Kyy, Kzz, Kyz, Kxz, Kxy;
       if (D2) {
         kern_at(a.K, 0, k, kzc, Kxx, Kyy, Kzz, Kyz, Kxz, Kxy);
-        kmul4(v[i][0][q], v[i][1][q], v[i][2][q], Kxx, Kyy, Kzz, Kyz);
+        kmul4_fma(v[i][0][q], v[i][1][q], v[i][2][q], Kxx, Kyy, Kzz, Kyz);
       } else {
         kern_at(a.K, k, kyc, kzc, Kxx, Kyy, Kzz, Kyz, Kxz, Kxy);
-        kmul6(v[i][0][q], v[i][1][q], v[i][2][q], Kxx, Kyy, Kzz, Kyz, Kxz, Kxy);
+        kmul6_fma(v[i][0][q], v[i][1][q], v[i][2][q], Kxx, Kyy, Kzz, Kyz, Kxz, Kxy);
       }
     }
   }
@@ -432,11 +432,14 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
     }
     sm[k * SIP + l] = v;
   }
+  __syncthreads();
+  tile_fft_fixed<M, NL, T, true, SIP, 1, true>(sm, tw);
   float lmax = 0.f;
   const int64_t g0 = (int64_t)r0 * N2;
   if (N2 == M) {
-    // open boundary along Z: the row has exactly M cells.  The epilogue's
-    // per-cell inputs are loaded before the transform.
+    // open boundary along Z: the row has exactly M cells.  Every per-cell
+    // input of this thread's cells is loaded before any is used, so the
+    // loads are in flight together.
     constexpr int CPT = (RT * M + T - 1) / T;
     EpiIn<MODE> in[CPT];
 #pragma unroll
@@ -444,8 +447,6 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
       int e = threadIdx.x + i * T;
       if (e < nr * M) epi_load<MODE>(ea, g0 + e, in[i]);
     }
-    __syncthreads();
-    tile_fft_fixed<M, NL, T, true, SIP, 1, true>(sm, tw);
 #pragma unroll
     for (int i = 0; i < CPT; i++) {
       int e = threadIdx.x + i * T;
@@ -458,8 +459,6 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
       epi_cell_in<MODE>(ea, g0 + e, hx, hy, hz, in[i], lmax);
     }
   } else {
-    __syncthreads();
-    tile_fft_fixed<M, NL, T, true, SIP, 1, true>(sm, tw);
     for (int e = threadIdx.x; e < nr * N2; e += T) {
       int r = e / N2, zz = e - r * N2;
       const float2* base = sm + (zz >> 1) * SIP + 3 * r;

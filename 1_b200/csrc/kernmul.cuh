@@ -54,3 +54,32 @@ __device__ __forceinline__ void kmul4(float2& mx, float2& my, float2& mz, float 
   mz = hz;
 }
 
+// The same products with fused multiply-adds, for the fused convolution
+// passes (their results are compared with the FP64 oracle within a
+// tolerance; the drop-in gpu_kernelmul6/4 keep the rounding above).
+__device__ __forceinline__ void kmul6_fma(float2& mx, float2& my, float2& mz, float Kxx, float Kyy, float Kzz,
+                                          float Kyz, float Kxz, float Kxy) {
+  float2 hx, hy, hz;
+  hx.x = fmaf(mz.x, Kxz, fmaf(my.x, Kxy, mx.x * Kxx));
+  hx.y = fmaf(mz.y, Kxz, fmaf(my.y, Kxy, mx.y * Kxx));
+  hy.x = fmaf(mz.x, Kyz, fmaf(my.x, Kyy, mx.x * Kxy));
+  hy.y = fmaf(mz.y, Kyz, fmaf(my.y, Kyy, mx.y * Kxy));
+  hz.x = fmaf(mz.x, Kzz, fmaf(my.x, Kyz, mx.x * Kxz));
+  hz.y = fmaf(mz.y, Kzz, fmaf(my.y, Kyz, mx.y * Kxz));
+  mx = hx;
+  my = hy;
+  mz = hz;
+}
+__device__ __forceinline__ void kmul4_fma(float2& mx, float2& my, float2& mz, float Kxx, float Kyy, float Kzz,
+                                          float Kyz) {
+  float2 hx, hy, hz;
+  hx.x = mx.x * Kxx;
+  hx.y = mx.y * Kxx;
+  hy.x = fmaf(mz.x, Kyz, my.x * Kyy);
+  hy.y = fmaf(mz.y, Kyz, my.y * Kyy);
+  hz.x = fmaf(mz.x, Kzz, my.x * Kyz);
+  hz.y = fmaf(mz.y, Kzz, my.y * Kyz);
+  mx = hx;
+  my = hy;
+  mz = hz;
+}

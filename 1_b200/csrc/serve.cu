@@ -41,6 +41,7 @@ struct Req {
   size_t footprint = 0;
   mmx_solver* s = nullptr;
   int state = MMX_REQ_QUEUED;
+  int slot = -1;  // index in the current batch
   int point = 0;
   long long steps = 0, point_steps = 0;
   int converged = 1;
@@ -228,7 +229,10 @@ extern "C" int mmx_server_pump(mmx_server* sv, int* n_active, int* n_queued) {
       if (sv->dirty || !sv->batch) {
         if (sv->batch) { mmx_batch_destroy(sv->batch); sv->batch = nullptr; }
         std::vector<mmx_solver*> ss;
-        for (Req* q : sv->active) ss.push_back(q->s);
+        for (Req* q : sv->active) {
+          q->slot = (int)ss.size();
+          ss.push_back(q->s);
+        }
         MMX_CHECK_RC(mmx_batch_create_from(ss.data(), n, &sv->batch));
         MMX_CHECK_RC(mmx_batch_use_graph(sv->batch, 1));
         sv->rebuilds++;
@@ -266,9 +270,10 @@ extern "C" int mmx_server_pump(mmx_server* sv, int* n_active, int* n_queued) {
       q->point_steps = 0;
       q->point++;
       if (q->point < q->r.npoints) {
-        // next field of the sweep: the batch regroups with the new Zeeman term
-        MMX_CHECK_RC(mmx_solver_set_hext(q->s, &q->fields[3 * (size_t)q->point]));
-        sv->dirty = true;
+        // next field of the sweep, written into the batch's tables in place
+        const float* h = &q->fields[3 * (size_t)q->point];
+        if (sv->cfg.batched && sv->batch && !sv->dirty) MMX_CHECK_RC(mmx_batch_set_hext(sv->batch, q->slot, h));
+        else MMX_CHECK_RC(mmx_solver_set_hext(q->s, h));
       } else {
         if (sv->cfg.keep_m) {
           q->m_final.resize(3 * (size_t)q->s->n);

@@ -48,7 +48,8 @@ SERVE_WORKLOADS = {
     # BASELINE serving configuration: Poisson 200 req/s, seed 5, relaxations
     # (alpha 1, stop at max torque < 1e-4) and 21-point sweeps of B along x
     # from -100 to +100 mT; a bounded sample of the stream's first requests.
-    "serve-fp32-rk4-mixed": dict(seed=5, rate=200.0, dt=1e-13, max_torque=1e-4, check_every=100, points=21),
+    # dt None: each request's stable RK4 step (1_b200.stable_dt)
+    "serve-fp32-rk4-mixed": dict(seed=5, rate=200.0, dt=None, max_torque=1e-4, check_every=100, points=21),
 }
 DEFAULT = "plain-fp32-heun-256x256x32"
 
@@ -276,7 +277,7 @@ def run_serve(args, name):
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": name, "requests": len(mine), "stream_requests": len(reqs),
-                       "rate_per_s": sw["rate"], "seed": sw["seed"], "dt_s": sw["dt"],
+                       "rate_per_s": sw["rate"], "seed": sw["seed"], "dt_s": sw["dt"] or "stable_dt per request",
                        "max_torque": sw["max_torque"], "check_every": sw["check_every"],
                        "sweep_points": sw["points"], "max_steps_per_point": args.serve_max_steps,
                        "sample": "the first %d requests of the stream, arriving in real time" % len(reqs)},

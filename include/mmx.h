@@ -136,6 +136,16 @@ mmx_solver* mmx_batch_instance(mmx_batch* b, int i);
 int mmx_batch_size(mmx_batch* b, int* count, long long* cells, int* launches_per_step);
 int mmx_batch_step(mmx_batch* b, int nsteps, cudaStream_t stream);
 int mmx_batch_use_graph(mmx_batch* b, int on);
+/* Changes the uniform Zeeman field of instance i in place (the batch's
+ * argument tables and graph stay valid); synchronous. */
+int mmx_batch_set_hext(mmx_batch* b, int i, const float hext[3]);
+/* Tile shapes of the batched Y passes are chosen by measurement: the first
+ * batch needing a line length times both compiled column-tile widths on its
+ * own spectrum buffers and keeps the faster for the process.  This lists
+ * the decisions so far: per entry rows[5] = {line length, inverse, width 0,
+ * width 1, chosen} and ms[2] = the two measured launch times; *n = entries
+ * (at most max are written). */
+int mmx_batch_tuning(int max, int* rows, float* ms, int* n);
 /* The maximum torque of every instance in the last RK4 step, gathered into
  * out (count floats; host when on_host != 0, asynchronous on 'stream'). */
 int mmx_batch_torques(mmx_batch* b, float* out, int on_host, cudaStream_t stream);

@@ -54,3 +54,19 @@ def test_batch_rk4_vs_oracle(eng, cuda):
         o.steps(10)
         assert np.abs(b.instances[i].get_m() - o.m()).max() < 1e-5
     b.close()
+
+
+def test_autotuner_times_both_column_tiles(eng, cuda):
+    cfgs = eng.batch_config(4, seed=9, solver="rk4", dt=5e-15)
+    b = eng.Batch([eng.mmx_params(**c) for c in cfgs])
+    tune = eng.batch_tuning()
+    b.close()
+    P1 = {2 * c["grid"][1] for c in cfgs if c["grid"][2] > 1}  # user y -> internal Y, padded (3D instances)
+    seen = {(t["L"], t["inverse"]) for t in tune}
+    for L in P1:
+        assert (L, False) in seen and (L, True) in seen
+    for t in tune:
+        assert t["ms"][0] > 0 and t["ms"][1] > 0
+        assert t["chosen"] in t["widths"]
+        faster = t["widths"][1] if t["ms"][1] < t["ms"][0] else t["widths"][0]
+        assert t["chosen"] == faster

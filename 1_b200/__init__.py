@@ -251,6 +251,7 @@ MMX = {
     "mmx_server_clock": (ctypes.c_double, [ctypes.c_void_p]),
     "mmx_server_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t),
                                         ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
+    "mmx_dft_tc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "mmx_reduce_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                          ctypes.c_void_p]),
     "mmx_face_kernel6": (ctypes.c_int, [c_int_p, c_int_p, ctypes.POINTER(ctypes.c_float), ctypes.c_int,

@@ -204,6 +204,13 @@ int mmx_server_release(mmx_server* sv, long long id);
 double mmx_server_clock(mmx_server* sv);
 int mmx_server_stats(mmx_server* sv, size_t* used_bytes, long long* chunks, long long* regroups);
 
+/* Precision form building block: batched complex DFTs of length 32 as one
+ * split-BF16 tensor-core GEMM (tcgen05) per 256 vectors: each operand is
+ * split into bfloat16 hi + lo and hi.hi + hi.lo + lo.hi is accumulated in
+ * FP32.  in/out: device arrays of nvec x 32 complex (float2); inverse != 0
+ * uses exp(+2 pi i jk / 32) (unnormalised).  Synchronous. */
+int mmx_dft_tc(const float2* in, float2* out, int nvec, int inverse, cudaStream_t stream);
+
 /* Allocation-free reduction.  No counterpart in the reference: a variant of
  * gpu_reduce (same operations, 1 add, 2 max, 3 max |x|, 4 min, 5 sum |x|)
  * for callers that cannot call cudaMalloc -- code running while a CUDA

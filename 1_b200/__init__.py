@@ -67,6 +67,7 @@ class MmxParams(ctypes.Structure):
         ("exch_type", ctypes.c_int),
         ("faithful", ctypes.c_int),
         ("accuracy", ctypes.c_int),
+        ("precision", ctypes.c_int),
     ]
 
 
@@ -340,7 +341,7 @@ def units(msat, aexch):
 
 
 def mmx_params(grid, cell, msat, aexch, alpha, bext=(0, 0, 0), solver="heun", dt=0.0, maxerror=0.0, anis=0,
-               k1=0.0, axis=(0, 0, 1), periodic=(0, 0, 0), faithful=1, exch_type=6):
+               k1=0.0, axis=(0, 0, 1), periodic=(0, 0, 0), faithful=1, exch_type=6, precision=0):
     """Builds mmx_params from the reference's user-level (SI, user x,y,z)
     inputs with the same float32 conversions as the Go driver."""
     u = units(msat, aexch)
@@ -365,6 +366,7 @@ def mmx_params(grid, cell, msat, aexch, alpha, bext=(0, 0, 0), solver="heun", dt
     p.exch_type = exch_type
     p.faithful = faithful
     p.accuracy = 8
+    p.precision = precision
     return p
 
 

@@ -617,6 +617,10 @@ static void batch_free(mmx_batch* b) {
 }
 
 static int batch_check(mmx_solver* s, int solver) {
+  if (s->p.precision) {
+    mmx_set_error("batched form: FP32 transforms only (precision = 0)");
+    return MMX_ERR_ARG;
+  }
   if (s->p.solver != solver || s->p.max_error != 0.f) {
     mmx_set_error("all instances of a batch must use the same fixed-step solver (Heun or RK4)");
     return MMX_ERR_ARG;

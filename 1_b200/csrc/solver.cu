@@ -386,8 +386,18 @@ static cudaError_t launch_xconv(mmx_solver* s, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+int mmx_yconv2d_tc_launch(float2* S, int64_t CS, int HZ, int N1, const float* kh, int64_t kcs, int* err,
+                          cudaStream_t st);
+int mmx_yconv2d_tc_prepare();
+
 static cudaError_t launch_yconv2d(mmx_solver* s, cudaStream_t st) {
   int P1 = s->P[1];
+  if (s->p.precision) {
+    ScopedPass sp(s, "yconv2d_tc", st);
+    int rc = mmx_yconv2d_tc_launch(s->S, s->CS, s->HZ, s->N[1], s->K.kh, s->K.cs,
+                                   reinterpret_cast<int*>(s->scratch + 15), st);
+    return rc == MMX_OK ? cudaSuccess : cudaErrorLaunchFailure;
+  }
   if (fx_ok(P1)) {
     ConvArgs a;
     a.S = s->S;
@@ -813,6 +823,11 @@ extern "C" int mmx_solver_create(const mmx_params* p, mmx_solver** out) {
     if (s->N[d] < 1) { delete s; mmx_set_error("size must be >= 1"); return MMX_ERR_SIZE; }
     s->P[d] = (s->N[d] > 1 && p->periodic[d] == 0) ? 2 * s->N[d] : s->N[d];
   }
+  if (p->precision && !(p->size[0] == 1 && s->P[1] == 1024 && s->N[1] == 512 && p->periodic[1] == 0)) {
+    delete s;
+    mmx_set_error("precision form: 2D films with Ny = 512 (padded 1024) only");
+    return MMX_ERR_SIZE;
+  }
   if (s->N[2] < 2 || s->N[1] < 2) {
     delete s;
     mmx_set_error("internal Y and Z sizes must be >= 2 (gpu_fft0.cu:124-126)");
@@ -892,6 +907,10 @@ extern "C" int mmx_solver_create(const mmx_params* p, mmx_solver** out) {
     s->K.cs = ocs;
   }
 #undef ALLOC
+  if (s->p.precision) {
+    rc = mmx_yconv2d_tc_prepare();
+    if (rc != MMX_OK) { solver_free(s); return rc; }
+  }
   *out = s;
   return MMX_OK;
 }
@@ -1030,6 +1049,11 @@ extern "C" int mmx_solver_avg_m(mmx_solver* s, float* out3, int on_host, cudaStr
 extern "C" int mmx_solver_state(mmx_solver* s, double* time, float* dt, float* max_torque, float* step_error,
                                 long long* steps) {
   if (!s) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  if (s->p.precision) {
+    int tc_err = 0;
+    MMX_TRY(cudaMemcpy(&tc_err, s->scratch + 15, sizeof(int), cudaMemcpyDeviceToHost));
+    if (tc_err) { mmx_set_error("tensor-core convolution: completion wait timed out"); return MMX_ERR_CUDA; }
+  }
   if (time) *time = s->time;
   if (dt) *dt = s->dt;
   if (max_torque) *max_torque = s->torque;

@@ -62,6 +62,8 @@ typedef struct mmx_params {
   int exch_type;        /* 6: six-neighbour exchange folded into the kernel; 0: none */
   int faithful;         /* 1: keep the reference's FSAL-after-reject reuse */
   int accuracy;         /* face-integral points per side (reference: 8) */
+  int precision;        /* 0: FP32 transforms; 1: split-BF16 tensor-core DFT
+                           GEMMs for the Y convolution (2D films, Ny = 512) */
 } mmx_params;
 
 typedef struct mmx_solver mmx_solver;

@@ -51,6 +51,13 @@ SERVE_WORKLOADS = {
     # dt None: each request's stable RK4 step (1_b200.stable_dt)
     "serve-fp32-rk4-mixed": dict(seed=5, rate=200.0, dt=None, max_torque=1e-4, check_every=100, points=21),
 }
+PRECISION_WORKLOADS = {
+    # BASELINE precision configuration: 512 x 512 x 1 film of 2 nm cells,
+    # Ms 8.6e5, A 1.3e-11, alpha 0.1, vortex-like m (seed 3), RK23 1e-5
+    "precision-bf16x3-rk23-512x512": dict(
+        grid=(512, 512, 1), cell=(2e-9, 2e-9, 2e-9), msat=8.6e5, aexch=1.3e-11, alpha=0.1, solver="rk23",
+        maxerror=1e-5, seed=3),
+}
 DEFAULT = "plain-fp32-heun-256x256x32"
 
 
@@ -311,6 +318,95 @@ def run_serve(args, name):
         print(json.dumps(line), flush=True)
 
 
+def vortex_m(nx, ny, seed=3, core=2.5, noise=0.02):
+    """In-plane curl about the film centre, +z within `core` cells of it,
+    plus noise * N(0,1) per component (default_rng(seed)), normalised;
+    internal layout [3][1][ny][nx] (internal component C = user 2-C)."""
+    y, x = np.mgrid[0:ny, 0:nx].astype(np.float64)
+    x -= (nx - 1) / 2.0
+    y -= (ny - 1) / 2.0
+    r = np.hypot(x, y)
+    u = np.zeros((3, 1, ny, nx))
+    u[0, 0] = -y / np.maximum(r, 1e-12)
+    u[1, 0] = x / np.maximum(r, 1e-12)
+    inner = r <= core
+    u[0, 0][inner] = 0.0
+    u[1, 0][inner] = 0.0
+    u[2, 0][inner] = 1.0
+    u += noise * np.random.default_rng(seed).standard_normal(u.shape)
+    u /= np.sqrt((u * u).sum(axis=0, keepdims=True))
+    return np.ascontiguousarray(u[::-1]).astype(np.float32)
+
+
+def run_precision(args, name):
+    """The precision form against the FP32 form on the same film: RK23
+    steps per second of each, the split-precision field's error against the
+    FP64 oracle (one evaluation) and the two forms' difference after the
+    same simulated time."""
+    import torch
+    eng = importlib.import_module("1_b200")
+    w = PRECISION_WORKLOADS[name]
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    nx, ny, _ = w["grid"]
+    n = nx * ny
+    m0 = vortex_m(nx, ny, w["seed"])
+    kw = {k: w[k] for k in ("grid", "cell", "msat", "aexch", "alpha", "solver", "maxerror")}
+    stream = torch.cuda.Stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    res = {}
+    for prec in (1, 0):
+        s = eng.Solver(eng.mmx_params(**kw, precision=prec))
+        s.set_m(m0, sh)
+        s.normalize(sh)
+        s.step(args.warmup, sh)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.step(args.steps, sh)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        st = s.state()
+        # per-pass times
+        s.profile(True)
+        s.step(min(args.steps, 50), sh)
+        torch.cuda.synchronize()
+        times = s.pass_times()
+        s.profile(False)
+        res[prec] = dict(ms=ms, state=st, m=s.get_m(), passes={k: v[0] / v[1] for k, v in times.items()})
+        # field of the initial state for the FP64 comparison
+        mt = torch.from_numpy(m0).cuda()
+        ht = torch.zeros_like(mt)
+        s.field(ctypes.c_void_p(mt.data_ptr()), ctypes.c_void_p(ht.data_ptr()))
+        torch.cuda.synchronize()
+        res[prec]["h"] = ht.cpu().numpy()
+        s.close()
+    clk = clocks.stop()
+    import oracle as O  # the checker: FP64 field of the same state
+    h64 = O.OracleSim(O.make_cfg(**kw), m0, bits=64).heff(m0.astype(np.float64))
+    scale = float(np.abs(h64).max())
+    p, f = res[1], res[0]
+    value = n * args.steps / (p["ms"] / 1e3)
+    line = {"metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": p["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3 split, f32 accumulate", "data": "synthetic",
+            "config": {"workload": name, "grid": list(w["grid"]), "solver": "rk23", "maxerror": w["maxerror"],
+                       "init": "vortex, seed 3"},
+            "fp32_form": {"value": n * args.steps / (f["ms"] / 1e3), "ms_per_step": f["ms"] / args.steps,
+                          "passes_ms_per_launch": f["passes"]},
+            "passes_ms_per_launch": p["passes"],
+            "field_err_vs_fp64": {"split_bf16": float(np.abs(p["h"] - h64).max()) / scale,
+                                  "fp32": float(np.abs(f["h"] - h64).max()) / scale,
+                                  "norm": "max |h - h_fp64| / max |h_fp64|, one evaluation of the initial state"},
+            "gpu_launches": None, "clocks": clk}
+    # same number of adaptive steps: compare the states where both forms stand
+    line["after_steps"] = {"steps": args.warmup + args.steps, "time_split": p["state"]["time"],
+                           "time_fp32": f["state"]["time"],
+                           "max_abs_dm_split_vs_fp32": float(np.abs(p["m"] - f["m"]).max())}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, w, name):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -454,7 +550,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT,
-                    choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) + sorted(SERVE_WORKLOADS))
+                    choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) + sorted(SERVE_WORKLOADS) +
+                    sorted(PRECISION_WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--requests", type=int, default=16, help="serving: requests of the stream to run")
     ap.add_argument("--serve-max-steps", type=int, default=0, help="serving: step cap per relaxation (0: none)")
@@ -465,6 +562,9 @@ def main():
             import torch.distributed as dist
             dist.init_process_group("gloo", init_method="env://")
         run_serve(args, args.workload)
+        return
+    if args.workload in PRECISION_WORKLOADS:
+        run_precision(args, args.workload)
         return
     if args.workload in BATCH_WORKLOADS:
         run_batch(args, args.workload)

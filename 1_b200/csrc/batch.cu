@@ -200,7 +200,7 @@ template <int M>
 static cudaError_t run_zr2c(const Launch& l, cudaStream_t st) {
   constexpr int RT = fx_rows(M, 1);
   constexpr int T = fx_threads(RT * M);
-  size_t smem = sizeof(float2) * (size_t)odd_pitch(RT) * M;
+  size_t smem = sizeof(float2) * (size_t)RT * row_pitch(M);
   if (l.flag) {
     set_smem(kb_zr2c<M, RT, T, true>, smem);
     kb_zr2c<M, RT, T, true><<<l.blocks, T, smem, st>>>((const BZr2c*)l.args, l.starts, l.nseg);
@@ -214,7 +214,7 @@ template <int M, int MODE>
 static cudaError_t run_zinv_mode(const Launch& l, cudaStream_t st) {
   constexpr int RT = fx_rows(M, 3);
   constexpr int T = fx_threads(3 * RT * M);
-  size_t smem = sizeof(float2) * (size_t)odd_pitch(3 * RT) * M;
+  size_t smem = sizeof(float2) * (size_t)3 * RT * row_pitch(M);
   set_smem(kb_zinv<M, RT, T, MODE>, smem);
   kb_zinv<M, RT, T, MODE><<<l.blocks, T, smem, st>>>((const ZinvArgs*)l.args, l.starts, l.nseg);
   return cudaGetLastError();

@@ -140,3 +140,56 @@ template <int L, int TK, int T, bool LFAST, int SI, int SL, bool INV>
 __device__ __forceinline__ void tile_fft_fixed(float2* s, const float2* tw) {
   MidStages<L, 0, n_stages(L), TK, T, LFAST, SI, SL, INV>::run(s, tw);
 }
+
+// ---------------------------------------------------------------------
+// Row tiles: NLINES lines of L stored row-major with one float2 of padding
+// per 16 (element (l, i) at l*PITCH + i + i/16), butterflies mapped with j
+// fastest.  The first stage of a Z transform then reads 16 consecutive
+// elements of one row per half-warp straight from global memory
+// (coalesced), and every shared-memory stage (stride-R first-stage writes
+// included) is free of bank conflicts.
+// ---------------------------------------------------------------------
+__host__ __device__ constexpr int row_pitch(int L) {
+  return (L + L / 16) % 16 == 0 ? L + L / 16 + 8 : L + L / 16;
+}
+__device__ __forceinline__ int padi(int i) { return i + (i >> 4); }
+
+template <int L, int R, int NS, int NLINES, int T, int PITCH>
+__device__ __forceinline__ void stage_rows(float2* s, const float2* tw, bool inv) {
+  using S = St<L, R, NS, NLINES, T, false>;
+  float2 v[S::NB][R];
+#pragma unroll
+  for (int i = 0; i < S::NB; i++) {
+    if (!S::valid(i)) continue;
+    int l, j;
+    S::lj(i, l, j);
+#pragma unroll
+    for (int q = 0; q < R; q++) v[i][q] = s[l * PITCH + padi(S::in_idx(j, q))];
+    S::twiddle(v[i], j, tw, inv);
+    dft<R>(v[i], inv);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < S::NB; i++) {
+    if (!S::valid(i)) continue;
+    int l, j;
+    S::lj(i, l, j);
+#pragma unroll
+    for (int q = 0; q < R; q++) s[l * PITCH + padi(S::out_idx(j, q))] = v[i][q];
+  }
+  __syncthreads();
+}
+
+// stages [ST, ST1) of a forward or inverse transform of a row tile
+template <int L, int ST, int ST1, int NLINES, int T, int PITCH, bool INV>
+struct MidRows {
+  __device__ __forceinline__ static void run(float2* s, const float2* tw) {
+    if constexpr (ST < ST1) {
+      constexpr int R = INV ? inv_radix(L, ST) : fwd_radix(L, ST);
+      constexpr int NS = INV ? inv_span(L, ST) : fwd_span(L, ST);
+      stage_rows<L, R, NS, NLINES, T, PITCH>(s, tw, INV);
+      MidRows<L, ST + 1, ST1, NLINES, T, PITCH, INV>::run(s, tw);
+    }
+  }
+};
+

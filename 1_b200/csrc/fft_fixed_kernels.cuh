@@ -290,7 +290,8 @@ __device__ __forceinline__ void zr2c_body(const float* __restrict__ src, float2*
   __shared__ float2 tw[M];
   __shared__ int64_t roff_s[RT], soff_s[RT];
   extern __shared__ float2 sm[];
-  constexpr int SIP = odd_pitch(RT);
+  constexpr int PITCH = row_pitch(M);
+  constexpr int NST = n_stages(M);
   load_twiddles<M, T>(tw, z.f.tw, z.f.tws);
   const int r0 = bx * RT;
   const int nl = min(RT, z.nrows - r0);
@@ -303,33 +304,47 @@ __device__ __forceinline__ void zr2c_body(const float* __restrict__ src, float2*
   __syncthreads();
   const float dt = COMB ? *cb.dt : 0.f;
   const int nreal = z.n_real;
-#pragma unroll 4
-  for (int e = threadIdx.x; e < RT * M; e += T) {
-    int l = e / M, n = e % M;
-    float a = 0.f, b = 0.f;
-    if (l < nl) {
-      int64_t roff = roff_s[l];
-      int i0 = 2 * n;
-      if (COMB) {
-        if (i0 < nreal) { a = zcomb_value(cb, dt, roff + i0); cb.out[roff + i0] = a; }
-        if (i0 + 1 < nreal) { b = zcomb_value(cb, dt, roff + i0 + 1); cb.out[roff + i0 + 1] = b; }
-      } else if (vec2 && i0 + 1 < nreal) {
-        float2 p = __ldg(reinterpret_cast<const float2*>(src + roff + i0));
-        a = p.x;
-        b = p.y;
-      } else {
-        if (i0 < nreal) a = src[roff + i0];
-        if (i0 + 1 < nreal) b = src[roff + i0 + 1];
+  // first stage straight from global memory: butterfly j of row l reads the
+  // pairs (x_2n, x_2n+1), n = j + q M/R0 (zero past the data)
+  constexpr int R0 = fwd_radix(M, 0);
+  using S0 = St<M, R0, 1, RT, T, false>;
+#pragma unroll
+  for (int i = 0; i < S0::NB; i++) {
+    if (!S0::valid(i)) continue;
+    int l, j;
+    S0::lj(i, l, j);
+    float2 v[R0];
+#pragma unroll
+    for (int q = 0; q < R0; q++) {
+      const int n = S0::in_idx(j, q);
+      float a = 0.f, b = 0.f;
+      if (l < nl) {
+        const int64_t roff = roff_s[l];
+        const int i0 = 2 * n;
+        if (COMB) {
+          if (i0 < nreal) { a = zcomb_value(cb, dt, roff + i0); cb.out[roff + i0] = a; }
+          if (i0 + 1 < nreal) { b = zcomb_value(cb, dt, roff + i0 + 1); cb.out[roff + i0 + 1] = b; }
+        } else if (vec2 && i0 + 1 < nreal) {
+          float2 p = __ldg(reinterpret_cast<const float2*>(src + roff + i0));
+          a = p.x;
+          b = p.y;
+        } else {
+          if (i0 < nreal) a = src[roff + i0];
+          if (i0 + 1 < nreal) b = src[roff + i0 + 1];
+        }
       }
+      v[q] = make_float2(a, b);
     }
-    sm[n * SIP + l] = make_float2(a, b);
+    dft<R0>(v, false);
+#pragma unroll
+    for (int q = 0; q < R0; q++) sm[l * PITCH + padi(S0::out_idx(j, q))] = v[q];
   }
   __syncthreads();
-  tile_fft_fixed<M, RT, T, true, SIP, 1, false>(sm, tw);
+  MidRows<M, 1, NST, RT, T, PITCH, false>::run(sm, tw);
   for (int e = threadIdx.x; e < nl * (M + 1); e += T) {
     int l = e / (M + 1), k = e - l * (M + 1);
-    float2 Zk = sm[(k == M ? 0 : k) * SIP + l];
-    float2 Zm = sm[(k == 0 ? 0 : M - k) * SIP + l];
+    float2 Zk = sm[l * PITCH + padi(k == M ? 0 : k)];
+    float2 Zm = sm[l * PITCH + padi(k == 0 ? 0 : M - k)];
     float2 E = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
     float2 O = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
     float2 w = tw[0];
@@ -405,7 +420,8 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
   __shared__ int64_t rbase_s[RT];
   extern __shared__ float2 sm[];
   constexpr int NL = 3 * RT;
-  constexpr int SIP = odd_pitch(NL);
+  constexpr int PITCH = row_pitch(M);
+  constexpr int NST = n_stages(M);
   const float2* __restrict__ S = za.S;
   const float2* __restrict__ twP = za.twP;
   const int P1 = za.P1, HZ = za.HZ, nrows = za.nrows;
@@ -421,19 +437,29 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
     rbase_s[threadIdx.x] = ((int64_t)x * P1 + y) * HZ;
   }
   __syncthreads();
-#pragma unroll 4
-  for (int e = threadIdx.x; e < NL * M; e += T) {
-    int l = e / M, k = e % M;
-    int r = l / 3, c = l - 3 * r;
-    float2 v = make_float2(0.f, 0.f);
-    if (r < nr) {
-      const float2* row = S + c * CS + rbase_s[r];
-      v = c2r_pre(row[k], row[M - k], k, M, twP);
+  // first inverse stage straight from global memory: line l = 3 r + c,
+  // butterfly j combines bins k = j + q M/R0 (each after the C2R split)
+  constexpr int R0 = inv_radix(M, 0);
+  using S0 = St<M, R0, 1, NL, T, false>;
+#pragma unroll
+  for (int i = 0; i < S0::NB; i++) {
+    if (!S0::valid(i)) continue;
+    int l, j;
+    S0::lj(i, l, j);
+    const int r = l / 3, c = l - 3 * r;
+    float2 v[R0];
+    const float2* row = S + c * CS + rbase_s[r < nr ? r : 0];
+#pragma unroll
+    for (int q = 0; q < R0; q++) {
+      const int k = S0::in_idx(j, q);
+      v[q] = (r < nr) ? c2r_pre(row[k], row[M - k], k, M, twP) : make_float2(0.f, 0.f);
     }
-    sm[k * SIP + l] = v;
+    dft<R0>(v, true);
+#pragma unroll
+    for (int q = 0; q < R0; q++) sm[l * PITCH + padi(S0::out_idx(j, q))] = v[q];
   }
   __syncthreads();
-  tile_fft_fixed<M, NL, T, true, SIP, 1, true>(sm, tw);
+  MidRows<M, 1, NST, NL, T, PITCH, true>::run(sm, tw);
   float lmax = 0.f;
   const int64_t g0 = (int64_t)r0 * N2;
   if (N2 == M) {
@@ -452,19 +478,19 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
       int e = threadIdx.x + i * T;
       if (e >= nr * M) continue;
       int r = e / M, zz = e % M;
-      const float2* base = sm + (zz >> 1) * SIP + 3 * r;
+      const float2* base = sm + 3 * r * PITCH + padi(zz >> 1);
       float hx = (zz & 1) ? base[0].y : base[0].x;
-      float hy = (zz & 1) ? base[1].y : base[1].x;
-      float hz = (zz & 1) ? base[2].y : base[2].x;
+      float hy = (zz & 1) ? base[PITCH].y : base[PITCH].x;
+      float hz = (zz & 1) ? base[2 * PITCH].y : base[2 * PITCH].x;
       epi_cell_in<MODE>(ea, g0 + e, hx, hy, hz, in[i], lmax);
     }
   } else {
     for (int e = threadIdx.x; e < nr * N2; e += T) {
       int r = e / N2, zz = e - r * N2;
-      const float2* base = sm + (zz >> 1) * SIP + 3 * r;
+      const float2* base = sm + 3 * r * PITCH + padi(zz >> 1);
       float hx = (zz & 1) ? base[0].y : base[0].x;
-      float hy = (zz & 1) ? base[1].y : base[1].x;
-      float hz = (zz & 1) ? base[2].y : base[2].x;
+      float hy = (zz & 1) ? base[PITCH].y : base[PITCH].x;
+      float hz = (zz & 1) ? base[2 * PITCH].y : base[2 * PITCH].x;
       epi_cell<MODE>(ea, g0 + e, hx, hy, hz, lmax);
     }
   }
@@ -532,7 +558,7 @@ template <int M, bool COMB>
 cudaError_t fx_launch_zr2c(const float* src, float2* dst, const ZPass& z, const ZComb& cb, cudaStream_t st) {
   constexpr int RT = fx_rows(M, 1);
   constexpr int T = fx_threads(RT * M);
-  size_t smem = sizeof(float2) * (size_t)odd_pitch(RT) * M;
+  size_t smem = sizeof(float2) * (size_t)RT * row_pitch(M);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_zr2c_fx<M, RT, T, COMB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   // 8-byte loads when every row starts at an even float offset
   int vec2 = (z.ld_real % 2 == 0) && (z.comp_stride_real % 2 == 0) && (((uintptr_t)src & 7) == 0);
@@ -555,7 +581,7 @@ cudaError_t fx_launch_zinv(const float2* S, const float2* twz, const float2* twP
                            const EpiArgs& ea, cudaStream_t st) {
   constexpr int RT = fx_rows(M, 3);
   constexpr int T = fx_threads(3 * RT * M);
-  size_t smem = sizeof(float2) * (size_t)odd_pitch(3 * RT) * M;
+  size_t smem = sizeof(float2) * (size_t)3 * RT * row_pitch(M);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_zinv_fx<M, RT, T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   ZinvArgs za;
   za.S = S;

@@ -225,11 +225,14 @@ struct YconvTc {
   int* err;
 };
 
-__device__ __forceinline__ void put_split(unsigned char* hi, unsigned char* lo, uint32_t off, float v) {
-  __nv_bfloat16 h, l;
-  dtc::split_bf16(v, h, l);
-  *reinterpret_cast<__nv_bfloat16*>(hi + off) = h;
-  *reinterpret_cast<__nv_bfloat16*>(lo + off) = l;
+// (re, im) at K positions 2i, 2i+1 of a vector: adjacent bfloat16s, one
+// 32-bit store into each of the hi and lo tiles
+__device__ __forceinline__ void put_split2(unsigned char* hi, unsigned char* lo, uint32_t off, float2 v) {
+  __nv_bfloat162 h, l;
+  dtc::split_bf16(v.x, h.x, l.x);
+  dtc::split_bf16(v.y, h.y, l.y);
+  *reinterpret_cast<__nv_bfloat162*>(hi + off) = h;
+  *reinterpret_cast<__nv_bfloat162*>(lo + off) = l;
 }
 
 // (re, im) of this lane's accumulator element and its partner lane's
@@ -278,8 +281,7 @@ __global__ void __launch_bounds__(YT) k_yconv2d_tc(YconvTc a) {
     float2 v = make_float2(0.f, 0.f);
     if (y < a.N1 && kz < HZ) v = a.S[c * a.CS + (int64_t)y * HZ + kz];
     int vec = 32 * (3 * kzl + c) + n2;
-    put_split(x_hi, x_lo, dtc::kmajor_off(vec, 2 * n1, 64), v.x);
-    put_split(x_hi, x_lo, dtc::kmajor_off(vec, 2 * n1 + 1, 64), v.y);
+    put_split2(x_hi, x_lo, dtc::kmajor_off(vec, 2 * n1, 64), v);
   }
   const uint32_t tbase = 0;  // set after the allocation is visible
   (void)tbase;
@@ -317,17 +319,17 @@ __global__ void __launch_bounds__(YT) k_yconv2d_tc(YconvTc a) {
   // rows: (k1, ri); columns: (col, n2).  twiddle W1024^(n2 k1) -> F2 operand (col, k1) x (n2, ri)
   if (ok) {
     const int k1 = hi_idx;
-    for (int c8 = 0; c8 < YNV; c8 += 8) {
-      float v[8];
-      dtc::tmem_ld8(tw_addr + c8, v);
+    for (int c8 = 0; c8 < YNV; c8 += 32) {
+      float v[32];
+      dtc::tmem_ld32(tw_addr + c8, v);
       dtc::tmem_wait_ld();
 #pragma unroll
-      for (int q = 0; q < 8; q++) {
+      for (int q = 0; q < 32; q++) {
         int col = (c8 + q) >> 5, n2 = (c8 + q) & 31;
         float2 z = pair_ri(v[q], ri);
         float2 w = tw[(n2 * k1) & (YL - 1)];
         float2 t = make_float2(fmaf(z.x, w.x, -z.y * w.y), fmaf(z.x, w.y, z.y * w.x));
-        if (lane < 16) put_split(x_hi, x_lo, dtc::kmajor_off(32 * col + k1, 2 * n2 + ri, 64), ri ? t.y : t.x);
+        if (lane < 16 && ri == 0) put_split2(x_hi, x_lo, dtc::kmajor_off(32 * col + k1, 2 * n2, 64), t);
       }
     }
   }
@@ -357,10 +359,10 @@ __global__ void __launch_bounds__(YT) k_yconv2d_tc(YconvTc a) {
           float2 hx = make_float2(mx.x * Kxx, mx.y * Kxx);
           float2 hy = make_float2(fmaf(mz.x, Kyz, my.x * Kyy), fmaf(mz.y, Kyz, my.y * Kyy));
           float2 hz = make_float2(fmaf(mz.x, Kzz, my.x * Kyz), fmaf(mz.y, Kzz, my.y * Kyz));
-          if (lane < 16) {
-            put_split(x_hi, x_lo, dtc::kmajor_off(32 * (3 * kzl + 0) + k1, 2 * k2 + ri, 64), ri ? hx.y : hx.x);
-            put_split(x_hi, x_lo, dtc::kmajor_off(32 * (3 * kzl + 1) + k1, 2 * k2 + ri, 64), ri ? hy.y : hy.x);
-            put_split(x_hi, x_lo, dtc::kmajor_off(32 * (3 * kzl + 2) + k1, 2 * k2 + ri, 64), ri ? hz.y : hz.x);
+          if (lane < 16 && ri == 0) {
+            put_split2(x_hi, x_lo, dtc::kmajor_off(32 * (3 * kzl + 0) + k1, 2 * k2, 64), hx);
+            put_split2(x_hi, x_lo, dtc::kmajor_off(32 * (3 * kzl + 1) + k1, 2 * k2, 64), hy);
+            put_split2(x_hi, x_lo, dtc::kmajor_off(32 * (3 * kzl + 2) + k1, 2 * k2, 64), hz);
           }
         }
       }
@@ -372,18 +374,18 @@ __global__ void __launch_bounds__(YT) k_yconv2d_tc(YconvTc a) {
   // rows: (n2, ri); columns: (col, k1).  twiddle W1024^(-n2 k1) -> I2 operand (col, n2) x (k1, ri)
   if (ok) {
     const int n2 = hi_idx;
-    for (int c8 = 0; c8 < YNV; c8 += 8) {
-      float v[8];
-      dtc::tmem_ld8(tw_addr + c8, v);
+    for (int c8 = 0; c8 < YNV; c8 += 32) {
+      float v[32];
+      dtc::tmem_ld32(tw_addr + c8, v);
       dtc::tmem_wait_ld();
 #pragma unroll
-      for (int q = 0; q < 8; q++) {
+      for (int q = 0; q < 32; q++) {
         int col = (c8 + q) >> 5, k1 = (c8 + q) & 31;
         float2 z = pair_ri(v[q], ri);
         float2 w = tw[(n2 * k1) & (YL - 1)];
         // z * conj(w)
         float2 t = make_float2(fmaf(z.x, w.x, z.y * w.y), fmaf(z.y, w.x, -z.x * w.y));
-        if (lane < 16) put_split(x_hi, x_lo, dtc::kmajor_off(32 * col + n2, 2 * k1 + ri, 64), ri ? t.y : t.x);
+        if (lane < 16 && ri == 0) put_split2(x_hi, x_lo, dtc::kmajor_off(32 * col + n2, 2 * k1, 64), t);
       }
     }
   }
@@ -393,12 +395,12 @@ __global__ void __launch_bounds__(YT) k_yconv2d_tc(YconvTc a) {
   // rows: (n1, ri); columns: (col, n2); y = 32 n1 + n2 < N1 stored
   if (ok && warp < 2) {
     const int n1 = hi_idx;
-    for (int c8 = 0; c8 < YNV; c8 += 8) {
-      float v[8];
-      dtc::tmem_ld8(tw_addr + c8, v);
+    for (int c8 = 0; c8 < YNV; c8 += 32) {
+      float v[32];
+      dtc::tmem_ld32(tw_addr + c8, v);
       dtc::tmem_wait_ld();
 #pragma unroll
-      for (int q = 0; q < 8; q++) {
+      for (int q = 0; q < 32; q++) {
         int col = (c8 + q) >> 5, n2 = (c8 + q) & 31;
         float2 z = pair_ri(v[q], ri);
         int c = col % 3, kzl = col / 3;

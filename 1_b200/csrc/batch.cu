@@ -54,11 +54,11 @@ __global__ void __launch_bounds__(T) kb_col(const BCol* __restrict__ a, const in
   const BCol& c = a[s];
   col_body<L, TK, T, INV>(c.src, c.dst, c.cp, t % c.ntx, t / c.ntx);
 }
-template <int L, int TK, int T, bool D2>
+template <int L, int TK, int T, bool D2, bool HALF>
 __global__ void __launch_bounds__(T) kb_conv(const ConvArgs* __restrict__ a, const int* __restrict__ starts,
                                              int nseg) {
   int s = find_seg(starts, nseg, blockIdx.x);
-  conv_body<L, TK, T, D2>(a[s], blockIdx.x - starts[s]);
+  conv_body<L, TK, T, D2, HALF>(a[s], blockIdx.x - starts[s]);
 }
 template <int M, int RT, int T, bool COMB>
 __global__ void __launch_bounds__(T) kb_zr2c(const BZr2c* __restrict__ a, const int* __restrict__ starts, int nseg) {
@@ -187,13 +187,16 @@ static cudaError_t run_conv(const Launch& l, cudaStream_t st) {
   constexpr int NBF = TKP * (L / fwd_radix(L, n_stages(L) - 1));
   constexpr int T = NBF < 64 ? 64 : (NBF > 512 ? 512 : ((NBF + 31) / 32) * 32);
   size_t smem = sizeof(float2) * (size_t)odd_pitch(3 * TKP) * L;
+  // variant 1: every instance of the launch has its data in the lower half
+#define KB_CONV_(D2, HALF)                                                                              \
+  set_smem(kb_conv<L, TKP, T, D2, HALF>, smem);                                                         \
+  kb_conv<L, TKP, T, D2, HALF><<<l.blocks, T, smem, st>>>((const ConvArgs*)l.args, l.starts, l.nseg);
   if (l.flag) {
-    set_smem(kb_conv<L, TKP, T, true>, smem);
-    kb_conv<L, TKP, T, true><<<l.blocks, T, smem, st>>>((const ConvArgs*)l.args, l.starts, l.nseg);
+    if (l.variant) { KB_CONV_(true, true) } else { KB_CONV_(true, false) }
   } else {
-    set_smem(kb_conv<L, TKP, T, false>, smem);
-    kb_conv<L, TKP, T, false><<<l.blocks, T, smem, st>>>((const ConvArgs*)l.args, l.starts, l.nseg);
+    if (l.variant) { KB_CONV_(false, true) } else { KB_CONV_(false, false) }
   }
+#undef KB_CONV_
   return cudaGetLastError();
 }
 template <int M>
@@ -573,6 +576,9 @@ static int build_eval(mmx_batch* b, std::vector<Launch>& out, int mode, bool com
         t.push_back(conv_tiles(g.first, c.ncols));
       }
       if ((rc = add_launch(b, out, L_CONV, g.first, d2, a, t)) != MMX_OK) return rc;
+      bool half = true;
+      for (const ConvArgs& c : a) half = half && 2 * c.n_data == g.first;
+      out.back().variant = half ? 1 : 0;
     }
   }
   // Y inverse (3D)

@@ -110,6 +110,54 @@ __device__ __forceinline__ void Radix<16>::dft(float2* v, bool inv) {
   }
 }
 
+// Radix-R DFTs whose upper half of inputs is zero (a zero-padded line's
+// first stage): the zero terms are never added.
+template <int R>
+__device__ __forceinline__ void dft_half(float2* v, bool inv) {
+  Radix<R>::dft(v, inv);
+}
+template <>
+__device__ __forceinline__ void dft_half<8>(float2* v, bool inv) {
+  // DFT4 of [a, b, 0, 0] = (a + b, a + W4 b, a - b, a - W4 b)
+  float2 mb = mul_mi(v[2], inv), md = mul_mi(v[3], inv);
+  float2 e[4] = {cadd(v[0], v[2]), cadd(v[0], mb), csub(v[0], v[2]), csub(v[0], mb)};
+  float2 o[4] = {cadd(v[1], v[3]), cadd(v[1], md), csub(v[1], v[3]), csub(v[1], md)};
+  const float h = 0.70710678118654752440f;
+  float2 w1 = inv ? make_float2(h, h) : make_float2(h, -h);
+  float2 w3 = inv ? make_float2(-h, h) : make_float2(-h, -h);
+  float2 o1 = cmul(o[1], w1);
+  float2 o2 = mul_mi(o[2], inv);
+  float2 o3 = cmul(o[3], w3);
+  v[0] = cadd(e[0], o[0]);
+  v[4] = csub(e[0], o[0]);
+  v[1] = cadd(e[1], o1);
+  v[5] = csub(e[1], o1);
+  v[2] = cadd(e[2], o2);
+  v[6] = csub(e[2], o2);
+  v[3] = cadd(e[3], o3);
+  v[7] = csub(e[3], o3);
+}
+template <>
+__device__ __forceinline__ void dft_half<16>(float2* v, bool inv) {
+  float2 e[8], o[8];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    e[k] = v[2 * k];
+    o[k] = v[2 * k + 1];
+  }
+  dft_half<8>(e, inv);
+  dft_half<8>(o, inv);
+  const float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f, h = 0.70710678118654752440f;
+  const float wr[8] = {1.f, c1, h, s1, 0.f, -s1, -h, -c1};
+  const float wi[8] = {0.f, s1, h, c1, 1.f, c1, h, s1};
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    float2 t = k == 0 ? o[0] : k == 4 ? mul_mi(o[4], inv) : cmul(o[k], make_float2(wr[k], inv ? wi[k] : -wi[k]));
+    v[k] = cadd(e[k], t);
+    v[k + 8] = csub(e[k], t);
+  }
+}
+
 // Odd radices: direct DFT with constant twiddles cos/sin(2 pi k / R).
 template <int R>
 __device__ __forceinline__ void odd_dft(float2* v, bool inv, const float* c, const float* s) {

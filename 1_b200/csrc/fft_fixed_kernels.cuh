@@ -119,7 +119,10 @@ struct ConvArgs {
 template <int L, int R, int NS, int TK, int T>
 using St3 = St<L, R, NS, TK, T, true>;  // (t, j) butterflies, components looped inside
 
-template <int L, int TK, int T, bool D2>
+// HALF: the line holds data in its lower half only (n_data = L/2, the
+// open-boundary case): the first stage skips the zero half and the last
+// inverse stage computes only the stored half.
+template <int L, int TK, int T, bool D2, bool HALF>
 __device__ __forceinline__ void conv_body(const ConvArgs& a, int bx) {
   __shared__ float2 tw[L];
   extern __shared__ float2 sm[];
@@ -149,9 +152,11 @@ __device__ __forceinline__ void conv_body(const ConvArgs& a, int bx) {
 #pragma unroll
         for (int q = 0; q < R0; q++) {
           int idx = S0::in_idx(j, q);
-          v[i][c][q] = (idx < nd && t < nc) ? a.S[c * a.CS + idx * a.stride + col0 + t] : make_float2(0.f, 0.f);
+          v[i][c][q] = ((HALF ? q < R0 / 2 : idx < nd) && t < nc) ? a.S[c * a.CS + idx * a.stride + col0 + t]
+                                                                  : make_float2(0.f, 0.f);
         }
-        dft<R0>(v[i][c], false);
+        if (HALF) dft_half<R0>(v[i][c], false);
+        else dft<R0>(v[i][c], false);
       }
     }
   } else {
@@ -166,9 +171,11 @@ __device__ __forceinline__ void conv_body(const ConvArgs& a, int bx) {
 #pragma unroll
         for (int q = 0; q < R0; q++) {
           int idx = S0::in_idx(j, q);
-          u[i][c][q] = (idx < nd && t < nc) ? a.S[c * a.CS + idx * a.stride + col0 + t] : make_float2(0.f, 0.f);
+          u[i][c][q] = ((HALF ? q < R0 / 2 : idx < nd) && t < nc) ? a.S[c * a.CS + idx * a.stride + col0 + t]
+                                                                  : make_float2(0.f, 0.f);
         }
-        dft<R0>(u[i][c], false);
+        if (HALF) dft_half<R0>(u[i][c], false);
+        else dft<R0>(u[i][c], false);
 #pragma unroll
         for (int q = 0; q < R0; q++) sm[S0::out_idx(j, q) * NLP + c * TK + t] = u[i][c][q];
       }
@@ -226,7 +233,7 @@ __device__ __forceinline__ void conv_body(const ConvArgs& a, int bx) {
 #pragma unroll
         for (int q = 0; q < RL; q++) {
           int idx = SL::out_idx(j, q);
-          if (idx < nd && t < nc) a.S[c * a.CS + idx * a.stride + col0 + t] = v[i][c][q];
+          if ((HALF ? q < RL / 2 : idx < nd) && t < nc) a.S[c * a.CS + idx * a.stride + col0 + t] = v[i][c][q];
         }
       }
     }
@@ -266,16 +273,16 @@ __device__ __forceinline__ void conv_body(const ConvArgs& a, int bx) {
 #pragma unroll
         for (int q = 0; q < RI; q++) {
           int idx = SI::out_idx(j, q);
-          if (idx < nd && t < nc) a.S[c * a.CS + idx * a.stride + col0 + t] = w[q];
+          if ((HALF ? q < RI / 2 : idx < nd) && t < nc) a.S[c * a.CS + idx * a.stride + col0 + t] = w[q];
         }
       }
     }
   }
 }
 
-template <int L, int TK, int T, bool D2>
+template <int L, int TK, int T, bool D2, bool HALF>
 __global__ void __launch_bounds__(T) k_conv_fx(ConvArgs a) {
-  conv_body<L, TK, T, D2>(a, blockIdx.x);
+  conv_body<L, TK, T, D2, HALF>(a, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------
@@ -545,8 +552,15 @@ cudaError_t fx_launch_conv(const ConvArgs& a, cudaStream_t st) {
   constexpr int NBF = TKP * (L / fwd_radix(L, n_stages(L) - 1));
   constexpr int T = NBF < 64 ? 64 : (NBF > 512 ? 512 : ((NBF + 31) / 32) * 32);
   size_t smem = sizeof(float2) * (size_t)odd_pitch(3 * TKP) * L;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_conv_fx<L, TKP, T, D2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_conv_fx<L, TKP, T, D2><<<div_up(a.ncols, TKP), T, smem, st>>>(a);
+  if (2 * a.n_data == L) {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_conv_fx<L, TKP, T, D2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_conv_fx<L, TKP, T, D2, true><<<div_up(a.ncols, TKP), T, smem, st>>>(a);
+  } else {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_conv_fx<L, TKP, T, D2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_conv_fx<L, TKP, T, D2, false><<<div_up(a.ncols, TKP), T, smem, st>>>(a);
+  }
   return cudaGetLastError();
 }
 

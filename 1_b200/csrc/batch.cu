@@ -47,12 +47,12 @@ struct BFin {
   int64_t n;
 };
 
-template <int L, int TK, int T, bool INV>
+template <int L, int TK, int T, bool INV, bool HALF>
 __global__ void __launch_bounds__(T) kb_col(const BCol* __restrict__ a, const int* __restrict__ starts, int nseg) {
   int s = find_seg(starts, nseg, blockIdx.x);
   int t = blockIdx.x - starts[s];
   const BCol& c = a[s];
-  col_body<L, TK, T, INV>(c.src, c.dst, c.cp, t % c.ntx, t / c.ntx);
+  col_body<L, TK, T, INV, HALF>(c.src, c.dst, c.cp, t % c.ntx, t / c.ntx);
 }
 template <int L, int TK, int T, bool D2, bool HALF>
 __global__ void __launch_bounds__(T) kb_conv(const ConvArgs* __restrict__ a, const int* __restrict__ starts,
@@ -95,6 +95,7 @@ struct Launch {
   void* args;     // device array of per-instance argument structs
   int* starts;    // device array of tile offsets
   int variant = 0;  // tile shape (column passes: 0 = fx_col_tk, 1 = col_tk_alt)
+  int half = 0;     // column passes: every instance's data fill half the line
   size_t args_off = 0, starts_off = 0;  // offsets into the batch's table block
 };
 enum { L_ZR2C = 0, L_COL = 1, L_CONV = 2, L_ZINV = 3, L_FIN = 4 };
@@ -162,13 +163,15 @@ template <int L, int TK>
 static cudaError_t run_col_tk(const Launch& l, cudaStream_t st) {
   constexpr int T = fx_threads(TK * L);
   size_t smem = sizeof(float2) * (size_t)odd_pitch(TK) * L;
+#define KB_COL_(INV, HALF)                                                                        \
+  set_smem(kb_col<L, TK, T, INV, HALF>, smem);                                                    \
+  kb_col<L, TK, T, INV, HALF><<<l.blocks, T, smem, st>>>((const BCol*)l.args, l.starts, l.nseg);
   if (l.flag) {
-    set_smem(kb_col<L, TK, T, true>, smem);
-    kb_col<L, TK, T, true><<<l.blocks, T, smem, st>>>((const BCol*)l.args, l.starts, l.nseg);
+    if (l.half) { KB_COL_(true, true) } else { KB_COL_(true, false) }
   } else {
-    set_smem(kb_col<L, TK, T, false>, smem);
-    kb_col<L, TK, T, false><<<l.blocks, T, smem, st>>>((const BCol*)l.args, l.starts, l.nseg);
+    if (l.half) { KB_COL_(false, true) } else { KB_COL_(false, false) }
   }
+#undef KB_COL_
   return cudaGetLastError();
 }
 template <int L>
@@ -428,6 +431,14 @@ static void col_args(mmx_batch* b, int L, int inv, const std::vector<int>& ids, 
   }
 }
 
+// every instance of a column launch has its data in (forward) or keeps
+// (inverse) the lower half of the line
+static int col_half(int L, int inv, const std::vector<BCol>& a) {
+  for (const BCol& c : a)
+    if (2 * (inv ? c.cp.n_out : c.cp.n_in) != L) return 0;
+  return 1;
+}
+
 static float time_launch(const Launch& l, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1) {
   if (run_launch(l, st) != cudaSuccess) return -1.f;  // warm-up
   cudaEventRecord(e0, st);
@@ -470,6 +481,7 @@ static int add_col_launch(mmx_batch* b, std::vector<Launch>& out, int L, int inv
         col_args(b, L, inv, ids, v, a, t);
         if ((rc = add_launch_now(b, tmp, L_COL, L, inv, a, t)) != MMX_OK) break;
         tmp.back().variant = v;
+        tmp.back().half = col_half(L, inv, a);
         ms[v] = time_launch(tmp.back(), st, e0, e1);
       }
     }
@@ -487,6 +499,7 @@ static int add_col_launch(mmx_batch* b, std::vector<Launch>& out, int L, int inv
   col_args(b, L, inv, ids, variant, a, t);
   if ((rc = add_launch(b, out, L_COL, L, inv, a, t)) != MMX_OK) return rc;
   out.back().variant = variant;
+  out.back().half = col_half(L, inv, a);
   return MMX_OK;
 }
 

@@ -18,7 +18,9 @@ __host__ __device__ constexpr int odd_pitch(int lines) { return (lines % 2) ? li
 // Stage 0 loads from global (rows >= n_in are zero), the last stage stores
 // to global (only rows < n_out).
 // ---------------------------------------------------------------------
-template <int L, int TK, int T, bool INV>
+// HALF: forward, the input holds data in its lower half only (n_in = L/2);
+// inverse, only the lower half of the output is kept (n_out = L/2).
+template <int L, int TK, int T, bool INV, bool HALF>
 __device__ __forceinline__ void col_body(const float2* src, float2* dst, const ColPass& cp, int bx, int by) {
   __shared__ float2 tw[L];
   extern __shared__ float2 sm[];
@@ -41,9 +43,11 @@ __device__ __forceinline__ void col_body(const float2* src, float2* dst, const C
 #pragma unroll
     for (int q = 0; q < R0; q++) {
       int idx = S0::in_idx(j, q);
-      v[i][q] = (idx < n_in && l < nc) ? src[pbase + idx * sti + l] : make_float2(0.f, 0.f);
+      v[i][q] = (((HALF && !INV) ? q < R0 / 2 : idx < n_in) && l < nc) ? src[pbase + idx * sti + l]
+                                                                        : make_float2(0.f, 0.f);
     }
-    dft<R0>(v[i], INV);
+    if (HALF && !INV) dft_half<R0>(v[i], INV);
+    else dft<R0>(v[i], INV);
   }
   if constexpr (NST == 1) {
 #pragma unroll
@@ -54,7 +58,7 @@ __device__ __forceinline__ void col_body(const float2* src, float2* dst, const C
 #pragma unroll
       for (int q = 0; q < R0; q++) {
         int idx = S0::out_idx(j, q);
-        if (idx < n_out && l < nc) dst[pbase + idx * sti + l] = v[i][q];
+        if (((HALF && INV) ? q < R0 / 2 : idx < n_out) && l < nc) dst[pbase + idx * sti + l] = v[i][q];
       }
     }
   } else {
@@ -84,15 +88,15 @@ __device__ __forceinline__ void col_body(const float2* src, float2* dst, const C
 #pragma unroll
       for (int q = 0; q < RL; q++) {
         int idx = SL::out_idx(j, q);
-        if (idx < n_out && l < nc) dst[pbase + idx * sti + l] = w[i][q];
+        if (((HALF && INV) ? q < RL / 2 : idx < n_out) && l < nc) dst[pbase + idx * sti + l] = w[i][q];
       }
     }
   }
 }
 
-template <int L, int TK, int T, bool INV>
+template <int L, int TK, int T, bool INV, bool HALF>
 __global__ void __launch_bounds__(T) k_col_fx(const float2* src, float2* dst, ColPass cp) {
-  col_body<L, TK, T, INV>(src, dst, cp, blockIdx.x, blockIdx.y);
+  col_body<L, TK, T, INV, HALF>(src, dst, cp, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------
@@ -281,7 +285,7 @@ __device__ __forceinline__ void conv_body(const ConvArgs& a, int bx) {
 }
 
 template <int L, int TK, int T, bool D2, bool HALF>
-__global__ void __launch_bounds__(T) k_conv_fx(ConvArgs a) {
+__global__ void __launch_bounds__(T, (768 / T) > 0 ? (768 / T) : 1) k_conv_fx(ConvArgs a) {
   conv_body<L, TK, T, D2, HALF>(a, blockIdx.x);
 }
 
@@ -363,7 +367,14 @@ __device__ __forceinline__ void zr2c_body(const float* __restrict__ src, float2*
 }
 
 template <int M, int RT, int T, bool COMB>
-__global__ void __launch_bounds__(T) k_zr2c_fx(const float* __restrict__ src, float2* __restrict__ dst, ZPass z,
+#ifdef MMX_LB_Z
+#define ZR2C_MINB ((1536 / T) > 0 ? (1536 / T) : 1)
+#define ZINV_MINB ((1280 / T) > 0 ? (1280 / T) : 1)
+#else
+#define ZR2C_MINB 1
+#define ZINV_MINB 1
+#endif
+__global__ void __launch_bounds__(T, ZR2C_MINB) k_zr2c_fx(const float* __restrict__ src, float2* __restrict__ dst, ZPass z,
                                                ZComb cb, int vec2) {
   zr2c_body<M, RT, T, COMB>(src, dst, z, cb, vec2, blockIdx.x);
 }
@@ -505,7 +516,7 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
 }
 
 template <int M, int RT, int T, int MODE>
-__global__ void __launch_bounds__(T) k_zinv_fx(ZinvArgs za) {
+__global__ void __launch_bounds__(T, ZINV_MINB) k_zinv_fx(ZinvArgs za) {
   zinv_body<M, RT, T, MODE>(za, blockIdx.x);
 }
 
@@ -538,9 +549,15 @@ cudaError_t fx_launch_col(const float2* src, float2* dst, const ColPass& cp, cud
   constexpr int TK = fx_col_tk(L);
   constexpr int T = fx_threads(TK * L);
   size_t smem = sizeof(float2) * (size_t)odd_pitch(TK) * L;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_col_fx<L, TK, T, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 grid(div_up(cp.ncols, TK), cp.nplanes);
-  k_col_fx<L, TK, T, INV><<<grid, T, smem, st>>>(src, dst, cp);
+  const bool half = 2 * (INV ? cp.n_out : cp.n_in) == L;
+  if (half) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_col_fx<L, TK, T, INV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_col_fx<L, TK, T, INV, true><<<grid, T, smem, st>>>(src, dst, cp);
+  } else {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_col_fx<L, TK, T, INV, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_col_fx<L, TK, T, INV, false><<<grid, T, smem, st>>>(src, dst, cp);
+  }
   return cudaGetLastError();
 }
 

@@ -285,6 +285,9 @@ __device__ __forceinline__ void conv_body(const ConvArgs& a, int bx) {
 }
 
 template <int L, int TK, int T, bool D2, bool HALF>
+// at least 768 resident threads per SM (6 blocks of 128 for L = 64):
+// measured faster than the unconstrained 96-register build (5 blocks) and
+// than 7 or 8 blocks (register spills)
 __global__ void __launch_bounds__(T, (768 / T) > 0 ? (768 / T) : 1) k_conv_fx(ConvArgs a) {
   conv_body<L, TK, T, D2, HALF>(a, blockIdx.x);
 }
@@ -367,14 +370,7 @@ __device__ __forceinline__ void zr2c_body(const float* __restrict__ src, float2*
 }
 
 template <int M, int RT, int T, bool COMB>
-#ifdef MMX_LB_Z
-#define ZR2C_MINB ((1536 / T) > 0 ? (1536 / T) : 1)
-#define ZINV_MINB ((1280 / T) > 0 ? (1280 / T) : 1)
-#else
-#define ZR2C_MINB 1
-#define ZINV_MINB 1
-#endif
-__global__ void __launch_bounds__(T, ZR2C_MINB) k_zr2c_fx(const float* __restrict__ src, float2* __restrict__ dst, ZPass z,
+__global__ void __launch_bounds__(T) k_zr2c_fx(const float* __restrict__ src, float2* __restrict__ dst, ZPass z,
                                                ZComb cb, int vec2) {
   zr2c_body<M, RT, T, COMB>(src, dst, z, cb, vec2, blockIdx.x);
 }
@@ -516,7 +512,7 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
 }
 
 template <int M, int RT, int T, int MODE>
-__global__ void __launch_bounds__(T, ZINV_MINB) k_zinv_fx(ZinvArgs za) {
+__global__ void __launch_bounds__(T) k_zinv_fx(ZinvArgs za) {
   zinv_body<M, RT, T, MODE>(za, blockIdx.x);
 }
 
@@ -581,8 +577,11 @@ cudaError_t fx_launch_conv(const ConvArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// rows per Z tile: 2048 elements for the forward pass (smaller blocks, more
+// of them resident), 4096 for the three-component inverse pass
 __host__ __device__ constexpr int fx_rows(int M, int lines_per_row) {
-  return (4096 / (M * lines_per_row)) < 1 ? 1 : (4096 / (M * lines_per_row) > 32 ? 32 : 4096 / (M * lines_per_row));
+  return lines_per_row == 1 ? ((2048 / M) < 1 ? 1 : (2048 / M > 32 ? 32 : 2048 / M))
+                            : ((4096 / (M * lines_per_row)) < 1 ? 1 : (4096 / (M * lines_per_row) > 32 ? 32 : 4096 / (M * lines_per_row)));
 }
 
 template <int M, bool COMB>

@@ -225,6 +225,7 @@ MMX = {
     "mmx_solver_set_hext": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "mmx_solver_m_device": (ctypes.c_void_p, [ctypes.c_void_p]),
     "mmx_solver_use_graph": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "mmx_solver_device_control": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "mmx_solver_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "mmx_solver_pass_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                              ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
@@ -435,6 +436,10 @@ class Solver:
 
     def use_graph(self, on=True):
         _check(lib().mmx_solver_use_graph(self.h, 1 if on else 0))
+
+    def device_control(self, on=True):
+        """Adaptive RK: dt controller on the device; step(n) = n trials."""
+        _check(lib().mmx_solver_device_control(self.h, 1 if on else 0))
 
     def profile(self, on=True):
         _check(lib().mmx_solver_profile(self.h, 1 if on else 0))

@@ -657,6 +657,7 @@ static int batch_build(mmx_batch* b) {
   int rc = MMX_OK;
   b->hext_off.assign(b->inst.size(), std::vector<size_t>());
   for (mmx_solver* s : b->inst) {
+    s->spec_ready = 0;  // the batch's passes reuse the spectrum buffer
     // the stage kernels read dt from the instance's device scalar
     MMX_TRY(cudaMemcpy(s->scratch + 2, &s->dt, sizeof(float), cudaMemcpyHostToDevice));
     b->cells += s->n;

@@ -63,9 +63,11 @@ __device__ __forceinline__ void epi_load(const EpiArgs& ea, int64_t g, EpiIn<MOD
   }
 }
 
+// next: if not null, receives the cell's next stage input (Heun: m1est
+// after the predictor, m after the corrector)
 template <int MODE>
 __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float hx, float hy, float hz,
-                                            const EpiIn<MODE>& in, float& lmax);
+                                            const EpiIn<MODE>& in, float& lmax, float* next = nullptr);
 
 // cell g (index into one component), field (hx,hy,hz) from the convolution
 template <int MODE>
@@ -77,7 +79,7 @@ __device__ __forceinline__ void epi_cell(const EpiArgs& ea, int64_t g, float hx,
 
 template <int MODE>
 __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float hx, float hy, float hz,
-                                            const EpiIn<MODE>& in, float& lmax) {
+                                            const EpiIn<MODE>& in, float& lmax, float* next) {
     const int64_t n = ea.n;
     float mx = in.m[0], my = in.m[1], mz = in.m[2];
     llg_local(ea.lf, mx, my, mz, hx, hy, hz);
@@ -103,6 +105,7 @@ __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float 
       ea.out1[g] = ex;
       ea.out1[n + g] = ey;
       ea.out1[2 * n + g] = ez;
+      if (next) { next[0] = ex; next[1] = ey; next[2] = ez; }
     } else if (MODE == EPI_HEUN2) {
       // t = 0.5 t1 + 0.5 t0; m = normalize(m + t)   (adaptive_heun.go:148-154)
       float tx = FA(FM(0.5f, hx), FM(0.5f, in.a0[0]));
@@ -113,6 +116,7 @@ __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float 
       ea.out0[g] = nx;
       ea.out0[n + g] = ny;
       ea.out0[2 * n + g] = nz;
+      if (next) { next[0] = nx; next[1] = ny; next[2] = nz; }
       if (ea.err) {
         // error = maxabs(m1est - m)   (adaptive_heun.go:158-160)
         float d0 = fabsf(FA(mx, FM(-1.f, nx)));

@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(T) k_zc2r_fx(const float2* __restrict__ src, f
 
 // Inverse Z of the three components of RT spatial rows + the solver epilogue.
 struct ZinvArgs {
-  const float2* S;
+  float2* S;
   const float2* twz;
   const float2* twP;
   int P1, HZ;
@@ -428,7 +428,12 @@ struct ZinvArgs {
   EpiArgs ea;
 };
 
-template <int M, int RT, int T, int MODE>
+// FUSE (Heun modes, open Z boundary): after the epilogue the block's new
+// magnetisation rows (the next evaluation's input) are still in its shared
+// tile, so the block also runs the next forward Z transform on them and
+// writes the same spectrum rows it read -- the next evaluation needs no
+// separate forward Z pass and never re-reads m.
+template <int M, int RT, int T, int MODE, bool FUSE = false>
 __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
   __shared__ float2 tw[M];
   __shared__ int64_t rbase_s[RT];
@@ -436,7 +441,7 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
   constexpr int NL = 3 * RT;
   constexpr int PITCH = row_pitch(M);
   constexpr int NST = n_stages(M);
-  const float2* __restrict__ S = za.S;
+  const float2* S = za.S;  // not restrict: the fused variant writes these rows back
   const float2* __restrict__ twP = za.twP;
   const int P1 = za.P1, HZ = za.HZ, nrows = za.nrows;
   const int64_t CS = za.CS;
@@ -492,11 +497,63 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
       int e = threadIdx.x + i * T;
       if (e >= nr * M) continue;
       int r = e / M, zz = e % M;
-      const float2* base = sm + 3 * r * PITCH + padi(zz >> 1);
+      float2* base = sm + 3 * r * PITCH + padi(zz >> 1);
       float hx = (zz & 1) ? base[0].y : base[0].x;
       float hy = (zz & 1) ? base[PITCH].y : base[PITCH].x;
       float hz = (zz & 1) ? base[2 * PITCH].y : base[2 * PITCH].x;
-      epi_cell_in<MODE>(ea, g0 + e, hx, hy, hz, in[i], lmax);
+      if constexpr (FUSE) {
+        // the same 4-byte word that held this cell's field takes its new m
+        float nm[3];
+        epi_cell_in<MODE>(ea, g0 + e, hx, hy, hz, in[i], lmax, nm);
+        float* w = reinterpret_cast<float*>(base) + (zz & 1);
+        w[0] = nm[0];
+        w[2 * PITCH] = nm[1];
+        w[4 * PITCH] = nm[2];
+      } else {
+        epi_cell_in<MODE>(ea, g0 + e, hx, hy, hz, in[i], lmax);
+      }
+    }
+    if constexpr (FUSE) {
+      epi_flush_max<MODE>(ea, lmax);
+      __syncthreads();
+      // forward Z of the new rows: pairs n < M/2 hold the data, the rest of
+      // each line is padding (zero); then the R2C split into the spectrum
+      constexpr int F0 = fwd_radix(M, 0);
+      using SF = St<M, F0, 1, NL, T, false>;
+      float2 f[SF::NB][F0];
+#pragma unroll
+      for (int i = 0; i < SF::NB; i++) {
+        if (!SF::valid(i)) continue;
+        int l, j;
+        SF::lj(i, l, j);
+#pragma unroll
+        for (int q = 0; q < F0; q++)
+          f[i][q] = (q < F0 / 2) ? sm[l * PITCH + padi(SF::in_idx(j, q))] : make_float2(0.f, 0.f);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < SF::NB; i++) {
+        if (!SF::valid(i)) continue;
+        int l, j;
+        SF::lj(i, l, j);
+        dft_half<F0>(f[i], false);
+#pragma unroll
+        for (int q = 0; q < F0; q++) sm[l * PITCH + padi(SF::out_idx(j, q))] = f[i][q];
+      }
+      __syncthreads();
+      MidRows<M, 1, NST, NL, T, PITCH, false>::run(sm, tw);
+      for (int e = threadIdx.x; e < 3 * nr * (M + 1); e += T) {
+        int l = e / (M + 1), k = e - l * (M + 1);
+        int r = l / 3, c = l - 3 * r;
+        float2 Zk = sm[l * PITCH + padi(k == M ? 0 : k)];
+        float2 Zm = sm[l * PITCH + padi(k == 0 ? 0 : M - k)];
+        float2 E = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+        float2 O = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+        float2 w = (k == M) ? make_float2(-1.f, 0.f) : __ldg(&twP[k]);
+        float2 wo = cmul_f(w, O);
+        za.S[c * CS + rbase_s[r] + k] = make_float2(E.x + wo.x, E.y + wo.y);
+      }
+      return;
     }
   } else {
     for (int e = threadIdx.x; e < nr * N2; e += T) {
@@ -514,6 +571,10 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
 template <int M, int RT, int T, int MODE>
 __global__ void __launch_bounds__(T) k_zinv_fx(ZinvArgs za) {
   zinv_body<M, RT, T, MODE>(za, blockIdx.x);
+}
+template <int M, int RT, int T, int MODE>
+__global__ void __launch_bounds__(T) k_zinv_fwd_fx(ZinvArgs za) {
+  zinv_body<M, RT, T, MODE, true>(za, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------
@@ -614,7 +675,7 @@ cudaError_t fx_launch_zinv(const float2* S, const float2* twz, const float2* twP
   size_t smem = sizeof(float2) * (size_t)3 * RT * row_pitch(M);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_zinv_fx<M, RT, T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   ZinvArgs za;
-  za.S = S;
+  za.S = const_cast<float2*>(S);
   za.twz = twz;
   za.twP = twP;
   za.P1 = P1;
@@ -623,5 +684,26 @@ cudaError_t fx_launch_zinv(const float2* S, const float2* twz, const float2* twP
   za.nrows = nrows;
   za.ea = ea;
   k_zinv_fx<M, RT, T, MODE><<<div_up(nrows, RT), T, smem, st>>>(za);
+  return cudaGetLastError();
+}
+
+// inverse Z + Heun epilogue + the next evaluation's forward Z (k_zinv_fwd_fx)
+template <int M, int MODE>
+cudaError_t fx_launch_zinv_fwd(float2* S, const float2* twz, const float2* twP, int P1, int HZ, int64_t CS, int nrows,
+                               const EpiArgs& ea, cudaStream_t st) {
+  constexpr int RT = fx_rows(M, 3);
+  constexpr int T = fx_threads(3 * RT * M);
+  size_t smem = sizeof(float2) * (size_t)3 * RT * row_pitch(M);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_zinv_fwd_fx<M, RT, T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  ZinvArgs za;
+  za.S = S;
+  za.twz = twz;
+  za.twP = twP;
+  za.P1 = P1;
+  za.HZ = HZ;
+  za.CS = CS;
+  za.nrows = nrows;
+  za.ea = ea;
+  k_zinv_fwd_fx<M, RT, T, MODE><<<div_up(nrows, RT), T, smem, st>>>(za);
   return cudaGetLastError();
 }

@@ -453,15 +453,48 @@ static cudaError_t launch_zinv(mmx_solver* s, const EpiArgs& ea, cudaStream_t st
   return cudaGetLastError();
 }
 
+// inverse Z + Heun epilogue + the next evaluation's forward Z in one pass
+template <int MODE>
+static cudaError_t launch_zinv_fwd(mmx_solver* s, const EpiArgs& ea, cudaStream_t st) {
+  int M = s->P[2] / 2;
+  int nrows = s->N[0] * s->N[1];
+  ScopedPass sp(s, "zinv_epi_zfwd", st);
+  switch (M) {
+#define C_(L) \
+  case L: return fx_launch_zinv_fwd<L, MODE>(s->S, s->bp.twz, s->bp.twz, s->P[1], s->HZ, s->CS, nrows, ea, st);
+    FX_SIZES(C_)
+#undef C_
+  }
+  return cudaErrorInvalidValue;
+}
+
+// Fixed-step Heun with an open Z boundary and a compiled Z length: each
+// inverse-Z epilogue also produces the next evaluation's forward Z, so the
+// spectrum buffer holds zfwd(m) between steps (spec_ready).
+static bool heun_fused(const mmx_solver* s) {
+  int M = s->P[2] / 2;
+  return s->p.solver == MMX_SOLVER_HEUN && s->p.max_error == 0.f && s->N[2] == M && s->p.periodic[2] == 0 &&
+         fx_ok(M);
+}
+
+static cudaError_t conv_rest(mmx_solver* s, cudaStream_t st);
+
+static cudaError_t zfwd_only(mmx_solver* s, const float* m, cudaStream_t st) {
+  ZPass z = box_zpass(&s->bp, 3, s->N[0], s->n, s->CS);
+  ScopedPass sp(s, "zfwd", st);
+  return launch_z_r2c(m, s->S, z, st);
+}
+
 // forward part of the field evaluation: m -> S (after the kernel multiply)
 static cudaError_t conv_front(mmx_solver* s, const float* m, cudaStream_t st) {
+  cudaError_t e = zfwd_only(s, m, st);
+  if (e != cudaSuccess) return e;
+  return conv_rest(s, st);
+}
+
+// the passes after the forward Z: Y / kernel product (X) / inverse Y
+static cudaError_t conv_rest(mmx_solver* s, cudaStream_t st) {
   cudaError_t e;
-  {
-    ZPass z = box_zpass(&s->bp, 3, s->N[0], s->n, s->CS);
-    ScopedPass sp(s, "zfwd", st);
-    e = launch_z_r2c(m, s->S, z, st);
-    if (e != cudaSuccess) return e;
-  }
   if (s->is2d) return launch_yconv2d(s, st);
   {
     ColPass y;
@@ -518,16 +551,25 @@ static cudaError_t heun_step(mmx_solver* s, cudaStream_t st) {
   cudaError_t e;
   EpiArgs ea = solver_base_args(s);
   ea.dtg = dtg;
+  const bool fused = heun_fused(s);
   // predictor
-  e = conv_front(s, s->m, st);
+  if (!fused || !s->spec_ready) {
+    e = zfwd_only(s, s->m, st);
+    if (e != cudaSuccess) return e;
+  }
+  e = conv_rest(s, st);
   if (e != cudaSuccess) return e;
   ea.m_in = s->m;
   ea.out0 = s->t0;
   ea.out1 = s->m1;
-  e = launch_zinv<EPI_HEUN1>(s, ea, st);
+  e = fused ? launch_zinv_fwd<EPI_HEUN1>(s, ea, st) : launch_zinv<EPI_HEUN1>(s, ea, st);
   if (e != cudaSuccess) return e;
   // corrector
-  e = conv_front(s, s->m1, st);
+  if (!fused) {
+    e = zfwd_only(s, s->m1, st);
+    if (e != cudaSuccess) return e;
+  }
+  e = conv_rest(s, st);
   if (e != cudaSuccess) return e;
   ea.m_in = s->m1;
   ea.aux0 = s->t0;
@@ -539,7 +581,9 @@ static cudaError_t heun_step(mmx_solver* s, cudaStream_t st) {
     e = cudaMemsetAsync(s->scratch, 0, sizeof(float), st);
     if (e != cudaSuccess) return e;
   }
-  return launch_zinv<EPI_HEUN2>(s, ea, st);
+  e = fused ? launch_zinv_fwd<EPI_HEUN2>(s, ea, st) : launch_zinv<EPI_HEUN2>(s, ea, st);
+  s->spec_ready = fused ? 1 : 0;
+  return e;
 }
 
 // RK stage i: combine the stage input, transform, torque epilogue.
@@ -617,9 +661,13 @@ static cudaError_t rk_stage(mmx_solver* s, int i, cudaStream_t st, float* dt_dev
   return launch_zinv<EPI_TORQUE>(s, ea, st);
 }
 
+// renorm_reject: normalise m also when the step was rejected (the host
+// controller's end of a step whose every trial failed); the device
+// controller leaves m untouched on a rejected trial and retries.
 __global__ void k_finalize_accept(float* __restrict__ m, const float* __restrict__ mnew, int64_t n,
-                                  const int* __restrict__ accept) {
+                                  const int* __restrict__ accept, int renorm_reject = 1) {
   bool acc = *accept != 0;
+  if (!acc && !renorm_reject) return;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     float x, y, z;
     if (acc) { x = mnew[i]; y = mnew[n + i]; z = mnew[2 * n + i]; }
@@ -799,6 +847,9 @@ extern "C" int mmx_face_kernel6(const int P[3], const int periodic[3], const flo
 static void solver_free(mmx_solver* s) {
   if (!s) return;
   if (s->gexec) cudaGraphExecDestroy(s->gexec);
+  for (int g = 0; g < 2; g++)
+    if (s->dgraph[g]) cudaGraphExecDestroy(s->dgraph[g]);
+  cudaFree(s->rkdev);
   cudaFree(s->S);
   cudaFree(s->kh);
   cudaFree(s->m);
@@ -925,6 +976,7 @@ extern "C" int mmx_solver_set_m(mmx_solver* s, const float* m, int on_host, cuda
   MMX_TRY(cudaMemcpyAsync(s->m, m, sizeof(float) * 3 * s->n, on_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st));
   MMX_TRY(cudaStreamSynchronize(st));
   s->fsal_init = 0;
+  s->spec_ready = 0;
   return MMX_OK;
 }
 
@@ -937,6 +989,7 @@ extern "C" int mmx_solver_get_m(mmx_solver* s, float* m, int on_host, cudaStream
 
 extern "C" int mmx_solver_normalize(mmx_solver* s, cudaStream_t st) {
   if (!s) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  s->spec_ready = 0;
   k_normalize3<<<solver_grid_1d(s->n), 256, 0, st>>>(s->m, s->n);
   MMX_TRY(cudaGetLastError());
   return MMX_OK;
@@ -944,6 +997,7 @@ extern "C" int mmx_solver_normalize(mmx_solver* s, cudaStream_t st) {
 
 extern "C" int mmx_solver_field(mmx_solver* s, const float* m, float* h, cudaStream_t st) {
   if (!s || !m || !h) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  s->spec_ready = 0;
   cudaError_t e = conv_front(s, m, st);
   if (e == cudaSuccess) {
     EpiArgs ea = solver_base_args(s);
@@ -964,6 +1018,199 @@ static int step_once(mmx_solver* s, cudaStream_t st) {
     return MMX_OK;
   }
   return rk_step(s, st);
+}
+
+// ---------------------------------------------------------------------
+// Device-side controller of the adaptive RK solvers (mmx_solver_device_control).
+// One trial of RK.step (rk.go:279-445) is a fixed launch sequence captured
+// once as a CUDA graph: FSAL copy k0 <- k_last (a copy instead of the host
+// path's pointer swap), the stages (their dt read from device memory),
+// then a one-thread controller that applies rk.go's float32 rules --
+// factor = (maxErr/err)^(1/order) clamped to [0.01, 2], reject when
+// err > 2 maxErr, the min/max dt clamps -- accumulates the time in float64
+// and flags acceptance for the finalisation.  A rejected trial leaves m
+// untouched; the next replay retries with the reduced dt.  No host
+// synchronisation per step.
+// ---------------------------------------------------------------------
+struct RkDev {
+  double time;
+  float dt;
+  int accept;
+  long long accepted, trials;
+  float torque, err;
+  int bad;
+};
+
+__global__ void k_fsal_copy(float* __restrict__ k0, const float* __restrict__ klast, int64_t n3,
+                            const RkDev* __restrict__ dev, int faithful, float* __restrict__ torque) {
+  const bool copy = dev->accept || faithful;  // rk.go:311-315 (retry: faithful reuses the rejected k_last)
+  float lmax = 0.f;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n3; i += (int64_t)gridDim.x * blockDim.x) {
+    float v = copy ? klast[i] : k0[i];
+    if (copy) k0[i] = v;
+    lmax = fmaxf(lmax, fabsf(v));
+  }
+  for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(torque, lmax);
+}
+
+struct RkCtl {
+  float max_error, min_dm, max_dm, min_dt, max_dt, unit_time;
+  double inv_order;
+  int bounds;
+};
+
+// dt bounds from the maximum torque of stage 0 (rk.go:348-373)
+__global__ void k_rk_bounds(float* __restrict__ scratch, RkDev* __restrict__ dev, RkCtl c) {
+  float mt = scratch[1];
+  float dt = scratch[2];
+  float dm = __fmul_rn(dt, mt);
+  if (dm < c.min_dm) dt = __fdiv_rn(c.min_dm, mt);
+  if (__fmul_rn(dt, c.unit_time) < c.min_dt) dt = __fdiv_rn(c.min_dt, c.unit_time);
+  if (c.max_dm != 0.f && dm > c.max_dm) dt = __fdiv_rn(c.max_dm, mt);
+  if (c.max_dt != 0.f && __fmul_rn(dt, c.unit_time) > c.max_dt) dt = __fdiv_rn(c.max_dt, c.unit_time);
+  if (dt != dt) dev->bad = 1;
+  scratch[2] = dt;
+  dev->dt = dt;
+}
+
+// the error rule of rk.go:401-439 in float32; time in float64
+__global__ void k_rk_control(float* __restrict__ scratch, RkDev* __restrict__ dev, RkCtl c) {
+  const float err = scratch[0];
+  const float dt = scratch[2];
+  float factor = (float)pow((double)__fdiv_rn(c.max_error, err), c.inv_order);
+  if (factor > 2.f) factor = 2.f;
+  if (factor < 0.01f) factor = 0.01f;
+  float nd = __fmul_rn(dt, factor);
+  if (nd != nd || err != err) dev->bad = 1;
+  int acc = !(err > __fmul_rn(2.f, c.max_error));
+  if (acc) {
+    dev->time += (double)dt;
+    dev->accepted++;
+    if (__fmul_rn(nd, c.unit_time) < c.min_dt) nd = __fdiv_rn(c.min_dt, c.unit_time);
+    if (c.max_dt != 0.f && __fmul_rn(nd, c.unit_time) > c.max_dt) nd = __fdiv_rn(c.max_dt, c.unit_time);
+  }
+  dev->trials++;
+  dev->accept = acc;
+  dev->err = err;
+  dev->torque = scratch[1];
+  dev->dt = nd;
+  scratch[2] = nd;
+  reinterpret_cast<int*>(scratch)[3] = acc;
+}
+
+static RkCtl rk_ctl(const mmx_solver* s) {
+  RkCtl c;
+  c.max_error = s->p.max_error;
+  c.min_dm = s->p.min_dm;
+  c.max_dm = s->p.max_dm;
+  c.min_dt = s->p.min_dt;
+  c.max_dt = s->p.max_dt;
+  c.unit_time = s->p.unit_time;
+  c.inv_order = 1. / s->errorder;
+  c.bounds = s->p.min_dm != 0.f || s->p.max_dm != 0.f || s->p.min_dt != 0.f || s->p.max_dt != 0.f;
+  return c;
+}
+
+// one trial; first: stage 0 evaluated (no FSAL value yet)
+static cudaError_t rk_device_trial(mmx_solver* s, cudaStream_t st, bool first) {
+  float* dt_dev = s->scratch + 2;
+  const int* acc_dev = reinterpret_cast<const int*>(s->scratch + 3);
+  RkDev* dev = reinterpret_cast<RkDev*>(s->rkdev);
+  const RkCtl c = rk_ctl(s);
+  const int last = s->stages - 1;
+  cudaError_t e;
+  for (int i = 0; i < s->stages; i++) {
+    if (i == 0) {
+      if ((e = cudaMemsetAsync(s->scratch + 1, 0, sizeof(float), st)) != cudaSuccess) return e;
+      if (s->fsal && !first) {
+        k_fsal_copy<<<solver_grid_1d(3 * s->n), 256, 0, st>>>(s->kb[0], s->kb[last], 3 * s->n, dev, s->p.faithful,
+                                                              s->scratch + 1);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      } else if ((e = rk_stage(s, 0, st, dt_dev)) != cudaSuccess) {
+        return e;
+      }
+      if (c.bounds) {
+        k_rk_bounds<<<1, 1, 0, st>>>(s->scratch, dev, c);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      }
+      continue;
+    }
+    if (i == last && (e = cudaMemsetAsync(s->scratch, 0, sizeof(float), st)) != cudaSuccess) return e;
+    if ((e = rk_stage(s, i, st, dt_dev)) != cudaSuccess) return e;
+  }
+  k_rk_control<<<1, 1, 0, st>>>(s->scratch, dev, c);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_finalize_accept<<<solver_grid_1d(s->n), 256, 0, st>>>(s->m, s->mnew, s->n, acc_dev, 0);
+  return cudaGetLastError();
+}
+
+static int rk_device_download(mmx_solver* s) {
+  RkDev h;
+  // trials may be in flight on any stream (the graphs replay on the caller's)
+  MMX_TRY(cudaDeviceSynchronize());
+  MMX_TRY(cudaMemcpy(&h, s->rkdev, sizeof(h), cudaMemcpyDeviceToHost));
+  if (h.bad) { mmx_set_error("dt = NaN"); return MMX_ERR_NAN; }
+  s->time = h.time;
+  s->dt = h.dt;
+  s->steps = s->steps_base + h.accepted;
+  s->torque = h.torque;
+  s->step_error = h.err;
+  s->trials = h.trials;
+  return MMX_OK;
+}
+
+extern "C" int mmx_solver_device_control(mmx_solver* s, int on) {
+  if (!s) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  if (on && (!s->adaptive || s->p.solver == MMX_SOLVER_HEUN)) {
+    mmx_set_error("device control: adaptive RK solvers (rk12, rk23, rkck, rkdp) only");
+    return MMX_ERR_ARG;
+  }
+  if (on && !s->devctl) {
+    if (!s->rkdev && cudaMalloc(&s->rkdev, sizeof(RkDev)) != cudaSuccess) {
+      mmx_set_error("out of device memory");
+      return MMX_ERR_MEM;
+    }
+    RkDev h;
+    memset(&h, 0, sizeof(h));
+    h.time = s->time;
+    h.dt = s->dt;
+    h.accept = 1;
+    MMX_TRY(cudaMemcpy(s->rkdev, &h, sizeof(h), cudaMemcpyHostToDevice));
+    MMX_TRY(cudaMemcpy(s->scratch + 2, &s->dt, sizeof(float), cudaMemcpyHostToDevice));
+    s->steps_base = s->steps;
+    s->devctl = 1;
+  } else if (!on && s->devctl) {
+    MMX_CHECK_RC(rk_device_download(s));
+    s->devctl = 0;
+    s->fsal_init = 0;  // the host path starts its FSAL chain afresh
+  }
+  return MMX_OK;
+}
+
+// n trials, each one graph replay
+static int rk_device_steps(mmx_solver* s, int n, cudaStream_t st) {
+  for (int k = 0; k < n; k++) {
+    const int g = (s->fsal && s->fsal_init) ? 1 : 0;
+    if (!s->dgraph[g] || s->dgraph_stream[g] != st) {
+      if (s->dgraph[g]) { cudaGraphExecDestroy(s->dgraph[g]); s->dgraph[g] = nullptr; }
+      cudaStream_t cap = st;
+      bool own = false;
+      if (cap == 0) { MMX_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)); own = true; }
+      cudaGraph_t gr;
+      MMX_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+      cudaError_t e = rk_device_trial(s, cap, g == 0);
+      cudaError_t e2 = cudaStreamEndCapture(cap, &gr);
+      if (own) cudaStreamDestroy(cap);
+      if (e != cudaSuccess || e2 != cudaSuccess) { mmx_set_error("graph capture failed"); return MMX_ERR_CUDA; }
+      MMX_TRY(cudaGraphInstantiate(&s->dgraph[g], gr, 0));
+      cudaGraphDestroy(gr);
+      s->dgraph_stream[g] = st;
+    }
+    MMX_TRY(cudaGraphLaunch(s->dgraph[g], st));
+    s->fsal_init = 1;
+  }
+  return MMX_OK;
 }
 
 static bool rk_fixed(const mmx_solver* s) {
@@ -994,6 +1241,7 @@ static cudaError_t step_launches(mmx_solver* s, cudaStream_t st) {
 
 extern "C" int mmx_solver_step(mmx_solver* s, int nsteps, cudaStream_t st) {
   if (!s || nsteps < 0) { mmx_set_error("bad argument"); return MMX_ERR_ARG; }
+  if (s->devctl) return rk_device_steps(s, nsteps, st);
   bool graphable = s->use_graph && !s->profile &&
                    ((s->p.solver == MMX_SOLVER_HEUN && s->p.max_error == 0.f) || rk_fixed(s));
   if (graphable && s->p.solver != MMX_SOLVER_HEUN && s->dt_uploaded != s->dt) {
@@ -1005,6 +1253,12 @@ extern "C" int mmx_solver_step(mmx_solver* s, int nsteps, cudaStream_t st) {
     s->dt_uploaded = s->dt;
   }
   for (int k = 0; k < nsteps; k++) {
+    if (graphable && heun_fused(s) && !s->spec_ready) {
+      // the captured step expects the forward Z spectrum of m in S
+      cudaError_t e = zfwd_only(s, s->m, st);
+      if (e != cudaSuccess) { mmx_set_error(cudaGetErrorString(e)); return MMX_ERR_CUDA; }
+      s->spec_ready = 1;
+    }
     if (graphable) {
       if (!s->gexec || s->gstream != st) {
         if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
@@ -1049,6 +1303,7 @@ extern "C" int mmx_solver_avg_m(mmx_solver* s, float* out3, int on_host, cudaStr
 extern "C" int mmx_solver_state(mmx_solver* s, double* time, float* dt, float* max_torque, float* step_error,
                                 long long* steps) {
   if (!s) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  if (s->devctl) MMX_CHECK_RC(rk_device_download(s));
   if (s->p.precision) {
     int tc_err = 0;
     MMX_TRY(cudaMemcpy(&tc_err, s->scratch + 15, sizeof(int), cudaMemcpyDeviceToHost));

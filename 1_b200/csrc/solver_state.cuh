@@ -38,11 +38,18 @@ struct mmx_solver {
   float torque = 0, step_error = 0;
   long long steps = 0;
   int fsal_init = 0;
+  int spec_ready = 0;  // S holds the forward Z spectrum of m (fused Heun steps)
   float dt_uploaded = -1.f;  // dt last written to the device scalar by the graph path
   // tableau
   int stages = 0, fsal = 0, adaptive = 0;
   double errorder = 1;
   float a[RK_MAXS][RK_MAXS], b[RK_MAXS], b2[RK_MAXS], c[RK_MAXS];
+  // device-side adaptive controller (mmx_solver_device_control)
+  int devctl = 0;
+  void* rkdev = nullptr;
+  long long steps_base = 0, trials = 0;
+  cudaGraphExec_t dgraph[2] = {nullptr, nullptr};  // first trial / FSAL trials
+  cudaStream_t dgraph_stream[2] = {nullptr, nullptr};
   // graph
   int use_graph = 0;
   cudaGraphExec_t gexec = nullptr;

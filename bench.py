@@ -51,6 +51,12 @@ SERVE_WORKLOADS = {
     # dt None: each request's stable RK4 step (1_b200.stable_dt)
     "serve-fp32-rk4-mixed": dict(seed=5, rate=200.0, dt=None, max_torque=1e-4, check_every=100, points=21),
 }
+ADAPTIVE_WORKLOADS = {
+    # BASELINE configuration 1 as configured: RK23, max error 1e-5, 128 x 32 x 1
+    "plain-fp32-rk23-128x32x1": dict(
+        grid=(128, 32, 1), cell=(3.90625e-9, 3.90625e-9, 3e-9), msat=8.0e5, aexch=1.3e-11, alpha=0.02,
+        bext=(-24.6e-3, 4.3e-3, 0.0), solver="rk23", maxerror=1e-5, seed=1, init="tilted"),
+}
 PRECISION_WORKLOADS = {
     # BASELINE precision configuration: 512 x 512 x 1 film of 2 nm cells,
     # Ms 8.6e5, A 1.3e-11, alpha 0.1, vortex-like m (seed 3), RK23 1e-5
@@ -102,7 +108,10 @@ def pass_bytes(w):
     else:
         koct = 4 * (P1 // 2 + 1) * HZ * 4
         b = {"zfwd": 3 * n * 4 + zspec, "yconv2d": 2 * zspec + koct, "zinv_epi": zspec + heun_epi}
-    per_step = 2 * sum(b.values())
+    per_step = 2 * sum(b.values())  # the model's bytes per Heun step (separate passes)
+    # the fused pass of a fixed-step Heun run (inverse Z + epilogue + the next
+    # forward Z): the spectrum rows in and out, the Heun state, m not re-read
+    b["zinv_epi_zfwd"] = 2 * zspec + heun_epi
     state = 9 * n * 4 + (yspec if P0 > 1 else zspec) + koct
     return b, per_step / n, state
 
@@ -407,6 +416,59 @@ def run_precision(args, name):
     print(json.dumps(line), flush=True)
 
 
+def run_adaptive(args, name):
+    """RK23 on the small film: accepted steps per second with the host dt
+    controller (8 bytes read back per trial, as the reference's two
+    reductions per step) and with the device controller (graph-replayed
+    trials, one read-back at the end)."""
+    import torch
+    eng = importlib.import_module("1_b200")
+    w = ADAPTIVE_WORKLOADS[name]
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n = int(np.prod(w["grid"]))
+    m0 = seeded_m(w["grid"], w["seed"], w["init"])
+    kw = {k: w[k] for k in ("grid", "cell", "msat", "aexch", "alpha", "bext", "solver", "maxerror")}
+    stream = torch.cuda.Stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    clocks = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    out = {}
+    for mode in ("device", "host"):
+        s = eng.Solver(eng.mmx_params(**kw))
+        s.set_m(m0, sh)
+        s.normalize(sh)
+        if mode == "device":
+            s.device_control(True)
+        s.step(args.warmup, sh)
+        st0 = s.state()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.step(args.steps, sh)
+        e1.record(stream)
+        e1.synchronize()
+        wall = time.perf_counter() - t0
+        st1 = s.state()
+        acc = st1["steps"] - st0["steps"]
+        out[mode] = dict(ms=e0.elapsed_time(e1), wall=wall, accepted=acc, sim_time=st1["time"] - st0["time"],
+                         calls=args.steps)
+        s.close()
+    clk = clocks.stop()
+    d, h = out["device"], out["host"]
+    value = n * d["accepted"] / (d["ms"] / 1e3)
+    line = {"metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": 1,
+            "steps": d["accepted"], "warmup": args.warmup, "ms_per_step": d["ms"] / max(1, d["accepted"]),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": name, "grid": list(w["grid"]), "solver": "rk23", "maxerror": w["maxerror"],
+                       "controller": "device (graph per trial)"},
+            "device_controller": {"trials": d["calls"], "accepted": d["accepted"],
+                                  "accepted_steps_per_s": d["accepted"] / (d["ms"] / 1e3)},
+            "host_controller": {"accepted": h["accepted"], "accepted_steps_per_s": h["accepted"] / (h["ms"] / 1e3),
+                                "value": n * h["accepted"] / (h["ms"] / 1e3)},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, w, name):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -551,7 +613,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT,
                     choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) + sorted(SERVE_WORKLOADS) +
-                    sorted(PRECISION_WORKLOADS))
+                    sorted(PRECISION_WORKLOADS) + sorted(ADAPTIVE_WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--requests", type=int, default=16, help="serving: requests of the stream to run")
     ap.add_argument("--serve-max-steps", type=int, default=0, help="serving: step cap per relaxation (0: none)")
@@ -562,6 +624,9 @@ def main():
             import torch.distributed as dist
             dist.init_process_group("gloo", init_method="env://")
         run_serve(args, args.workload)
+        return
+    if args.workload in ADAPTIVE_WORKLOADS:
+        run_adaptive(args, args.workload)
         return
     if args.workload in PRECISION_WORKLOADS:
         run_precision(args, args.workload)

@@ -112,6 +112,14 @@ float* mmx_solver_torque_device(mmx_solver* s);
 
 /* Capture one step in a CUDA graph and replay it (fixed-step solvers). */
 int mmx_solver_use_graph(mmx_solver* s, int on);
+/* Adaptive RK solvers (rk12, rk23, rkck, rkdp): with on != 0 the dt
+ * controller runs on the device (rk.go:348-445 in float32, time in
+ * float64) and each mmx_solver_step unit is ONE TRIAL, replayed as a CUDA
+ * graph with no host synchronisation; a rejected trial leaves m unchanged
+ * and the next one retries with the reduced dt.  mmx_solver_state reads the
+ * device controller (time, dt, accepted steps).  Turning it off hands the
+ * state back to the host controller. */
+int mmx_solver_device_control(mmx_solver* s, int on);
 
 /* Per-pass timing with CUDA events on the step's stream: when on, each
  * kernel of the step is bracketed by events; mmx_solver_pass_times

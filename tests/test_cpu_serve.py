@@ -1,8 +1,9 @@
 """Host side of the serving form (no GPU): the seeded request stream, the
 sweep fields' float32 arithmetic (simhysteresis.go:18-24 then the
 ApplyStatic conversion, simfield.go:87-98), the footprint the admission
-control budgets with, and the instance partition across ranks."""
+control budgets with, and the submission checks."""
 import numpy as np
+import pytest
 
 
 def test_stream_is_seeded_and_poisson(eng):
@@ -60,3 +61,28 @@ def test_footprint_counts_resident_buffers(eng):
     small = eng.mmx_params(grid=(32, 32, 1), cell=(3e-9,) * 3, msat=8e5, aexch=1.3e-11, alpha=1.0, solver="rk4",
                            dt=1e-13)
     assert eng.footprint(small) < eng.footprint(p) / 50
+
+
+def test_server_admission_checks_on_the_host(eng):
+    """Submission is pure host logic: requests whose footprint exceeds the
+    device budget, non-RK4 solves and malformed sweeps are refused with a
+    status, before anything reaches a GPU."""
+    sv = eng.Server(batched=True, check_every=10, hbm_budget=1 << 20)  # 1 MiB: nothing fits
+    r = eng.serve_stream(1, seed=5)[0]
+    m0 = eng.stream_m0(r)
+    with pytest.raises(eng.MmxError, match="out of memory|budget"):
+        sv.submit(eng.mmx_params(**r["cfg"]), m0, r["fields"])
+    sv.close()
+    sv = eng.Server(batched=True, check_every=10, hbm_budget=1 << 40)
+    heun = dict(r["cfg"], solver="heun")
+    with pytest.raises(eng.MmxError, match="bad argument|RK4"):
+        sv.submit(eng.mmx_params(**heun), m0, r["fields"])
+    with pytest.raises(eng.MmxError):
+        sv.submit(eng.mmx_params(**r["cfg"]), m0, None, max_torque=0.0)
+    rid = sv.submit(eng.mmx_params(**r["cfg"]), m0, r["fields"])
+    res = sv.result(rid)
+    assert res["state"] == "queued" and res["points_done"] == 0 and res["t_admit"] < 0
+    assert res["footprint"] == eng.footprint(eng.mmx_params(**r["cfg"]))
+    with pytest.raises(eng.MmxError):
+        sv.release(rid)  # still in flight
+    sv.close()

@@ -154,3 +154,63 @@ def test_reference_library_parity(eng, cuda, kind):
     fused.step(100)
     assert np.abs(ref.m() - mine.m()).max() <= 1e-5
     assert np.abs(ref.m() - fused.get_m()).max() <= 1e-5
+
+
+def test_rk23_device_controller_matches_host(eng, cuda):
+    """The device-side dt controller (graph-replayed trials, no host sync)
+    takes the same accepted steps as the host controller of rk.go."""
+    cfg = dict(grid=(128, 32, 1), cell=(3.90625e-9, 3.90625e-9, 3e-9), msat=8.0e5, aexch=1.3e-11, alpha=0.02,
+               bext=(-24.6e-3, 4.3e-3, 0.0), solver="rk23", maxerror=1e-5)
+    m0 = O.seeded_m(cfg["grid"], 1, "tilted")
+    host = eng.Solver(eng.mmx_params(**cfg))
+    host.set_m(m0)
+    host.normalize()
+    host.step(30)
+    sh = host.state()
+    dev = eng.Solver(eng.mmx_params(**cfg))
+    dev.set_m(m0)
+    dev.normalize()
+    dev.device_control(True)
+    sd = dev.state()
+    for _ in range(300):
+        dev.step(1)
+        sd = dev.state()
+        if sd["steps"] >= 30:
+            break
+    assert sd["steps"] == 30
+    assert abs(sd["time"] - sh["time"]) <= 1e-9 * sh["time"], (sd["time"], sh["time"])
+    assert np.abs(dev.get_m() - host.get_m()).max() < 1e-6
+    # and runs on without host synchronisation: many trials, one read-back
+    dev.step(200)
+    s2 = dev.state()
+    assert s2["steps"] > 30 and s2["time"] > sd["time"]
+    host.close()
+    dev.close()
+
+
+def test_fused_heun_spectrum_reuse(eng, cuda):
+    """Fixed-step Heun runs its inverse-Z epilogue and the next forward Z in
+    one pass (the spectrum buffer carries zfwd(m) between steps).  Setting m
+    between steps, stepping through the graph or directly, and the primitive
+    path all agree."""
+    cfg = dict(grid=(32, 16, 8), cell=(4e-9, 4e-9, 4e-9), msat=1.1e6, aexch=1.5e-11, alpha=0.5, anis=1, k1=5e5,
+               axis=(0, 0, 1), solver="heun", dt=1e-14)
+    m0 = O.seeded_m(cfg["grid"], 2, "random")
+    a = eng.Solver(eng.mmx_params(**cfg))
+    a.set_m(m0)
+    a.normalize()
+    a.use_graph(True)
+    a.step(4)
+    mid = a.get_m()
+    a.set_m(mid)  # invalidates the carried spectrum
+    a.step(4)
+    b = eng.Solver(eng.mmx_params(**cfg))
+    b.set_m(m0)
+    b.normalize()
+    b.step(8)  # direct launches
+    assert np.abs(a.get_m() - b.get_m()).max() < 1e-6
+    o = O.OracleSim(O.make_cfg(**cfg), m0, bits=64)
+    o.steps(8)
+    assert np.abs(b.get_m() - o.m()).max() < 1e-5
+    a.close()
+    b.close()

@@ -180,13 +180,11 @@ static cudaError_t run_col(const Launch& l, cudaStream_t st) {
 }
 template <int L>
 static int conv_tk() {
-  constexpr int TK = L >= 2048 ? 1 : (1365 / L > 32 ? 32 : (1365 / L < 1 ? 1 : 1365 / L));
-  return TK >= 16 ? 16 : (TK >= 8 ? 8 : (TK >= 4 ? 4 : (TK >= 2 ? 2 : 1)));
+  return conv_tkp(L);
 }
 template <int L>
 static cudaError_t run_conv(const Launch& l, cudaStream_t st) {
-  constexpr int TK0 = L >= 2048 ? 1 : (1365 / L > 32 ? 32 : (1365 / L < 1 ? 1 : 1365 / L));
-  constexpr int TKP = TK0 >= 16 ? 16 : (TK0 >= 8 ? 8 : (TK0 >= 4 ? 4 : (TK0 >= 2 ? 2 : 1)));
+  constexpr int TKP = conv_tkp(L);
   constexpr int NBF = TKP * (L / fwd_radix(L, n_stages(L) - 1));
   constexpr int T = NBF < 64 ? 64 : (NBF > 512 ? 512 : ((NBF + 31) / 32) * 32);
   size_t smem = sizeof(float2) * (size_t)odd_pitch(3 * TKP) * L;

@@ -349,7 +349,9 @@ __device__ __forceinline__ void zr2c_body(const float* __restrict__ src, float2*
       }
       v[q] = make_float2(a, b);
     }
-    dft<R0>(v, false);
+    // open boundary (n_real = M): the upper half of the pairs is padding
+    if (nreal == M) dft_half<R0>(v, false);
+    else dft<R0>(v, false);
 #pragma unroll
     for (int q = 0; q < R0; q++) sm[l * PITCH + padi(S0::out_idx(j, q))] = v[q];
   }
@@ -597,6 +599,18 @@ static inline bool fx_ok(int L) {
 __host__ __device__ constexpr int fx_col_tk(int L) {
   return L >= 4096 ? 1 : L >= 1024 ? 4096 / L : (4096 / L < 16 ? 16 : (4096 / L > 32 ? 32 : 4096 / L));
 }
+// columns per convolution tile (a power of two): about 1365/L, at most 16
+// (16 columns measured faster than 8 for L = 64)
+__host__ __device__ constexpr int conv_tk_raw(int L) {
+  return L >= 2048 ? 1 : (1365 / L > 32 ? 32 : (1365 / L < 1 ? 1 : 1365 / L));
+}
+__host__ __device__ constexpr int conv_tkp(int L) {
+  return conv_tk_raw(L) >= 16 ? 16
+         : conv_tk_raw(L) >= 8            ? 8
+         : conv_tk_raw(L) >= 4            ? 4
+         : conv_tk_raw(L) >= 2            ? 2
+                                          : 1;
+}
 __host__ __device__ constexpr int fx_threads(int elems) {
   return elems / 16 < 64 ? 64 : (elems / 16 > 512 ? 512 : ((elems / 16 + 31) / 32) * 32);
 }
@@ -620,8 +634,7 @@ cudaError_t fx_launch_col(const float2* src, float2* dst, const ColPass& cp, cud
 
 template <int L, bool D2>
 cudaError_t fx_launch_conv(const ConvArgs& a, cudaStream_t st) {
-  constexpr int TK = L >= 2048 ? 1 : (1365 / L > 32 ? 32 : (1365 / L < 1 ? 1 : 1365 / L)) ;
-  constexpr int TKP = TK >= 16 ? 16 : (TK >= 8 ? 8 : (TK >= 4 ? 4 : (TK >= 2 ? 2 : 1)));
+  constexpr int TKP = conv_tkp(L);
   // one thread per (column, radix-8 butterfly): it owns the three components
   constexpr int NBF = TKP * (L / fwd_radix(L, n_stages(L) - 1));
   constexpr int T = NBF < 64 ? 64 : (NBF > 512 ? 512 : ((NBF + 31) / 32) * 32);

@@ -13,9 +13,11 @@
 // count.  In batched mode every pump advances ALL resident solves by one
 // chunk of check_every steps through one mmx_batch (one launch per pass and
 // line length, one CUDA graph per step), so requests that arrive while
-// others run join at the next chunk boundary and share the launches.  In
-// plain mode the same loop runs one solve at a time on the single-instance
-// solver: the baseline the batching is measured against.
+// others run join at the next chunk boundary and share the launches; when
+// at most two solves remain resident they step on their own solver graphs,
+// whose per-step latency is lower.  In plain mode the same loop runs
+// one solve at a time on the single-instance solver: the baseline the
+// batching is measured against.
 //
 // Determinism: a solve is admitted only at a chunk boundary and its stop
 // checks fall on multiples of check_every of its OWN step count, and a
@@ -69,6 +71,11 @@ struct mmx_server {
   float* avg_host = nullptr;  // pinned host, 3 per resident solve
   long long chunks = 0, rebuilds = 0;
 };
+
+// resident solves at or below which a batched server steps each solve on
+// its own graph (measured: two; with four, or with one stream per solve,
+// the served throughput was lower)
+static const int SOLO_MAX = 2;
 
 static double sv_clock(const mmx_server* sv) {
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - sv->t0).count();
@@ -225,7 +232,11 @@ extern "C" int mmx_server_pump(mmx_server* sv, int* n_active, int* n_queued) {
   const int n = (int)sv->active.size();
   if (n > 0) {
     MMX_CHECK_RC(sv_host_buffers(sv, n));
-    if (sv->cfg.batched) {
+    // with very few resident solves the batch's per-launch overhead
+    // outweighs its sharing: step them on their own solvers' graphs (the
+    // same kernels and arithmetic, so results do not change)
+    const bool solo = !sv->cfg.batched || n <= SOLO_MAX;
+    if (!solo) {
       if (sv->dirty || !sv->batch) {
         if (sv->batch) { mmx_batch_destroy(sv->batch); sv->batch = nullptr; }
         std::vector<mmx_solver*> ss;
@@ -241,9 +252,13 @@ extern "C" int mmx_server_pump(mmx_server* sv, int* n_active, int* n_queued) {
       MMX_CHECK_RC(mmx_batch_step(sv->batch, K, sv->st));
       MMX_CHECK_RC(mmx_batch_torques(sv->batch, sv->torques, 1, sv->st));
     } else {
-      mmx_solver* s = sv->active[0]->s;
-      MMX_CHECK_RC(mmx_solver_step(s, K, sv->st));
-      MMX_TRY(cudaMemcpyAsync(sv->torques, mmx_solver_torque_device(s), sizeof(float), cudaMemcpyDeviceToHost, sv->st));
+      for (int i = 0; i < n; i++) {
+        mmx_solver* s = sv->active[i]->s;
+        MMX_CHECK_RC(mmx_solver_use_graph(s, 1));
+        MMX_CHECK_RC(mmx_solver_step(s, K, sv->st));
+        MMX_TRY(cudaMemcpyAsync(sv->torques + i, mmx_solver_torque_device(s), sizeof(float), cudaMemcpyDeviceToHost,
+                                sv->st));
+      }
     }
     MMX_TRY(cudaStreamSynchronize(sv->st));
     sv->chunks++;

@@ -41,24 +41,24 @@ WORKLOADS = {
         bext=(-24.6e-3, 4.3e-3, 0.0), solver="heun", dt=1e-14, seed=1, init="tilted"),
 }
 BATCH_WORKLOADS = {
-    # BASELINE batching configuration: 256 instances, RK4, fixed dt 5e-15 s
+    # batching workload: 256 uneven instances (seed 4), RK4, fixed dt 5e-15 s
     "batch-fp32-rk4-256": dict(count=256, seed=4, solver="rk4", dt=5e-15),
 }
 SERVE_WORKLOADS = {
-    # BASELINE serving configuration: Poisson 200 req/s, seed 5, relaxations
+    # serving workload: Poisson stream of 200 req/s, seed 5, relaxations
     # (alpha 1, stop at max torque < 1e-4) and 21-point sweeps of B along x
     # from -100 to +100 mT; a bounded sample of the stream's first requests.
     # dt None: each request's stable RK4 step (1_b200.stable_dt)
     "serve-fp32-rk4-mixed": dict(seed=5, rate=200.0, dt=None, max_torque=1e-4, check_every=100, points=21),
 }
 ADAPTIVE_WORKLOADS = {
-    # BASELINE configuration 1 as configured: RK23, max error 1e-5, 128 x 32 x 1
+    # 128 x 32 x 1 thin film (standard-problem-4 geometry), RK23, max error 1e-5
     "plain-fp32-rk23-128x32x1": dict(
         grid=(128, 32, 1), cell=(3.90625e-9, 3.90625e-9, 3e-9), msat=8.0e5, aexch=1.3e-11, alpha=0.02,
         bext=(-24.6e-3, 4.3e-3, 0.0), solver="rk23", maxerror=1e-5, seed=1, init="tilted"),
 }
 PRECISION_WORKLOADS = {
-    # BASELINE precision configuration: 512 x 512 x 1 film of 2 nm cells,
+    # precision workload: 512 x 512 x 1 film of 2 nm cells,
     # Ms 8.6e5, A 1.3e-11, alpha 0.1, vortex-like m (seed 3), RK23 1e-5
     "precision-bf16x3-rk23-512x512": dict(
         grid=(512, 512, 1), cell=(2e-9, 2e-9, 2e-9), msat=8.6e5, aexch=1.3e-11, alpha=0.1, solver="rk23",

@@ -31,13 +31,13 @@ import oracle as O  # noqa: E402
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libgpukern_ref.so")
 
 CASES = {
-    # 2D film, BASELINE configuration 1 materials on a 64 x 16 x 1 grid
+    # 2D film: the 128 x 32 x 1 thin-film materials on a 64 x 16 x 1 grid
     "film2d": dict(cfg=dict(grid=(64, 16, 1), cell=(3.90625e-9, 3.90625e-9, 3e-9), msat=8.0e5, aexch=1.3e-11,
                             alpha=0.02, bext=(-24.6e-3, 4.3e-3, 0.0)),
                    seed=1, init="tilted",
                    runs=[("heun", dict(solver="heun", dt=2e-13), 50),
                          ("rk23", dict(solver="rk23", maxerror=1e-5), 20)]),
-    # 3D grid, BASELINE configuration 2 materials on a 16 x 16 x 8 grid
+    # 3D grid: the 256 x 256 x 32 workload's materials on a 16 x 16 x 8 grid
     "cube3d": dict(cfg=dict(grid=(16, 16, 8), cell=(4e-9, 4e-9, 4e-9), msat=1.1e6, aexch=1.5e-11, alpha=0.5,
                             anis=1, k1=5e5, axis=(0, 0, 1)),
                    seed=2, init="random",

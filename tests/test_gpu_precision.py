@@ -28,7 +28,7 @@ def test_dft_tc_vs_fp64(eng, cuda, inverse, nvec):
 
 
 def vortex_m(nx, ny, seed=3, core=2.5, noise=0.02):
-    """cfg3's vortex-like state, user (x,y,z) -> internal [3][1][ny][nx]:
+    """The 512 x 512 film's vortex-like state, user (x,y,z) -> internal [3][1][ny][nx]:
     in-plane curl about the centre, +z within `core` cells of it, plus
     noise * N(0,1) per component (default_rng(seed)), normalised."""
     y, x = np.mgrid[0:ny, 0:nx].astype(np.float64)
@@ -47,7 +47,7 @@ def vortex_m(nx, ny, seed=3, core=2.5, noise=0.02):
     return np.ascontiguousarray(u[::-1]).astype(np.float32)
 
 
-CFG3 = dict(grid=(512, 512, 1), cell=(2e-9, 2e-9, 2e-9), msat=8.6e5, aexch=1.3e-11, alpha=0.1)
+FILM512 = dict(grid=(512, 512, 1), cell=(2e-9, 2e-9, 2e-9), msat=8.6e5, aexch=1.3e-11, alpha=0.1)
 
 
 def test_precision_field_vs_fp64(eng, cuda):
@@ -56,7 +56,7 @@ def test_precision_field_vs_fp64(eng, cuda):
     m = vortex_m(512, 512)
     h = {}
     for prec in (0, 1):
-        s = eng.Solver(eng.mmx_params(**CFG3, solver="rk23", maxerror=1e-5, precision=prec))
+        s = eng.Solver(eng.mmx_params(**FILM512, solver="rk23", maxerror=1e-5, precision=prec))
         mt = torch.from_numpy(m).cuda().contiguous()
         ht = torch.zeros_like(mt)
         s.field(ctypes.c_void_p(mt.data_ptr()), ctypes.c_void_p(ht.data_ptr()))
@@ -64,7 +64,7 @@ def test_precision_field_vs_fp64(eng, cuda):
         s.state()  # raises if the tensor-core waits timed out
         h[prec] = ht.cpu().numpy()
         s.close()
-    o = O.OracleSim(O.make_cfg(**CFG3, solver="rk23", maxerror=1e-5), m, bits=64)
+    o = O.OracleSim(O.make_cfg(**FILM512, solver="rk23", maxerror=1e-5), m, bits=64)
     h64 = o.heff(m.astype(np.float64))
     scale = np.abs(h64).max()
     e32 = np.abs(h[0] - h64).max() / scale
@@ -76,13 +76,13 @@ def test_precision_field_vs_fp64(eng, cuda):
 def test_precision_steps_vs_fp64(eng, cuda):
     import oracle as O
     m = vortex_m(512, 512)
-    s = eng.Solver(eng.mmx_params(**CFG3, solver="rk4", dt=1e-13, precision=1))
+    s = eng.Solver(eng.mmx_params(**FILM512, solver="rk4", dt=1e-13, precision=1))
     s.set_m(m)
     s.normalize()
     s.step(10)
     s.state()
     got = s.get_m()
     s.close()
-    o = O.OracleSim(O.make_cfg(**CFG3, solver="rk4", dt=1e-13), m, bits=64)
+    o = O.OracleSim(O.make_cfg(**FILM512, solver="rk4", dt=1e-13), m, bits=64)
     o.steps(10)
     assert np.abs(got - o.m()).max() < 1e-4

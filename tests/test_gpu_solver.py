@@ -39,12 +39,12 @@ def test_face_kernel_bitexact(eng, cuda, N, cs, per):
     assert np.array_equal(out.cpu().numpy(), ref)
 
 
-def cfg1_like(grid=(32, 16, 1)):
+def thin_film_like(grid=(32, 16, 1)):
     return dict(grid=grid, cell=(3.90625e-9, 3.90625e-9, 3e-9), msat=8.0e5, aexch=1.3e-11, alpha=0.02,
                 bext=(-24.6e-3, 4.3e-3, 0.0))
 
 
-def cfg2_like(grid=(16, 16, 8)):
+def anis_cube_like(grid=(16, 16, 8)):
     return dict(grid=grid, cell=(4e-9, 4e-9, 4e-9), msat=1.1e6, aexch=1.5e-11, alpha=0.5, anis=1, k1=5e5,
                 axis=(0, 0, 1))
 
@@ -53,7 +53,7 @@ def cfg2_like(grid=(16, 16, 8)):
 def test_fused_field_vs_oracle(eng, cuda, kind):
     """h = demag + exchange + Zeeman + anisotropy of the fused pipeline vs
     the oracle's FP64 run of the same field evaluation."""
-    c = cfg1_like() if kind == "2d" else cfg2_like()
+    c = thin_film_like() if kind == "2d" else anis_cube_like()
     m = O.seeded_m(c["grid"], 1, "random")
     ocfg = O.make_cfg(**c, solver="heun", dt=1e-14)
     o64 = O.OracleSim(ocfg, m, bits=64)
@@ -75,7 +75,7 @@ def test_fused_field_vs_oracle(eng, cuda, kind):
 
 def test_driver_heff_vs_oracle(eng, cuda):
     """The Go-driver restatement over the drop-in ABI (primitive path)."""
-    c = cfg2_like((8, 12, 4))
+    c = anis_cube_like((8, 12, 4))
     m = O.seeded_m(c["grid"], 2, "random")
     ocfg = O.make_cfg(**c, solver="heun", dt=1e-14)
     o64 = O.OracleSim(ocfg, m, bits=64)
@@ -92,7 +92,7 @@ def test_driver_heff_vs_oracle(eng, cuda):
 
 @pytest.mark.parametrize("solver,steps", [("heun", 20), ("rk23", 8), ("rk4", 8)])
 def test_fused_steps_vs_oracle(eng, cuda, solver, steps):
-    c = cfg1_like((32, 8, 1)) if solver != "rk4" else cfg2_like((8, 8, 4))
+    c = thin_film_like((32, 8, 1)) if solver != "rk4" else anis_cube_like((8, 8, 4))
     kw = dict(solver=solver, dt=1e-14 if solver != "rk23" else 0.0, maxerror=1e-5 if solver == "rk23" else 0.0)
     m = O.seeded_m(c["grid"], 3, "tilted")
     o = O.OracleSim(O.make_cfg(**c, **kw), m, bits=64)
@@ -110,7 +110,7 @@ def test_fused_steps_vs_oracle(eng, cuda, solver, steps):
 def test_fused_vs_primitive_heun(eng, cuda):
     """Fused Heun (mmx_solver_step) and the drop-in primitive sequence the Go
     driver issues agree to rounding."""
-    c = cfg2_like((16, 8, 4))
+    c = anis_cube_like((16, 8, 4))
     m = O.seeded_m(c["grid"], 4, "random")
     kw = dict(solver="heun", dt=1e-14)
     o32 = O.OracleSim(O.make_cfg(**c, **kw), m, bits=32)
@@ -133,7 +133,7 @@ def test_reference_library_parity(eng, cuda, kind):
     """The reference's own libgpukern (cuFFT path) and the B200 engine, both
     driven by the same Go-driver restatement on identical seeded inputs:
     max |dm| per cell after a fixed-dt run."""
-    c = cfg1_like((64, 16, 1)) if kind == "2d" else cfg2_like((16, 16, 8))
+    c = thin_film_like((64, 16, 1)) if kind == "2d" else anis_cube_like((16, 16, 8))
     kw = dict(solver="heun", dt=1e-14 if kind == "3d" else 2e-13)
     m = O.seeded_m(c["grid"], 5, "tilted" if kind == "2d" else "random")
     o32 = O.OracleSim(O.make_cfg(**c, **kw), m, bits=32)

@@ -9,7 +9,8 @@
 // per-instance arguments by a binary search on the tile offsets.  With the
 // batch configuration's sizes (Nx, Ny in {32,48,64,96,128,192,256}, Nz in
 // {1,2,4}) a Runge-Kutta stage is at most ~35 launches whatever the number
-// of instances, and a whole step is captured in one CUDA graph.
+// of instances, and a whole step is captured in one CUDA graph whose edges
+// follow each instance's own chain of launches.
 #include <map>
 #include <mutex>
 #include <string.h>
@@ -96,6 +97,7 @@ struct Launch {
   int* starts;    // device array of tile offsets
   int variant = 0;  // tile shape (column passes: 0 = fx_col_tk, 1 = col_tk_alt)
   int half = 0;     // column passes: every instance's data fill half the line
+  std::vector<int> inst;  // instances this launch reads or writes (graph dependencies)
   size_t args_off = 0, starts_off = 0;  // offsets into the batch's table block
 };
 enum { L_ZR2C = 0, L_COL = 1, L_CONV = 2, L_ZINV = 3, L_FIN = 4 };
@@ -114,10 +116,8 @@ struct mmx_batch {
   int launches_per_step = 0;
   float** torque_ptrs = nullptr;  // RK4: per-instance max |k0| slots, cleared each step
   float* gather = nullptr;        // device staging of the gathered torques
-  // graph capture: the launches of one pass (one per line length) are
-  // independent and run as parallel branches
+  // graph capture: streams and events of the per-instance dependency DAG
   std::vector<cudaStream_t> par;
-  cudaEvent_t ev_fork = nullptr;
   std::vector<cudaEvent_t> ev_join;
   // every launch's argument and tile-offset tables live in one device block,
   // staged on the host while the launches are built
@@ -128,17 +128,6 @@ struct mmx_batch {
   std::vector<std::vector<size_t>> hext_off;
 };
 
-// pass of a launch within a field evaluation; launches of the same pass
-// touch disjoint instances
-static int phase_of(const Launch& l) {
-  switch (l.kind) {
-    case L_ZR2C: return 0;
-    case L_COL: return l.flag ? 3 : 1;
-    case L_CONV: return 2;
-    case L_ZINV: return 4;
-    default: return 5;
-  }
-}
 
 __global__ void kb_clear(float** p, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -498,6 +487,7 @@ static int add_col_launch(mmx_batch* b, std::vector<Launch>& out, int L, int inv
   if ((rc = add_launch(b, out, L_COL, L, inv, a, t)) != MMX_OK) return rc;
   out.back().variant = variant;
   out.back().half = col_half(L, inv, a);
+  out.back().inst = ids;
   return MMX_OK;
 }
 
@@ -553,6 +543,7 @@ static int build_eval(mmx_batch* b, std::vector<Launch>& out, int mode, bool com
       t.push_back(div_up(z.z.nrows, zrows_per_tile(g.first, 1)));
     }
     if ((rc = add_launch(b, out, L_ZR2C, g.first, comb ? 1 : 0, a, t)) != MMX_OK) return rc;
+    out.back().inst = g.second;
   }
   // Y forward (3D)
   for (auto& g : byP1_3d)
@@ -587,6 +578,7 @@ static int build_eval(mmx_batch* b, std::vector<Launch>& out, int mode, bool com
         t.push_back(conv_tiles(g.first, c.ncols));
       }
       if ((rc = add_launch(b, out, L_CONV, g.first, d2, a, t)) != MMX_OK) return rc;
+      out.back().inst = g.second;
       bool half = true;
       for (const ConvArgs& c : a) half = half && 2 * c.n_data == g.first;
       out.back().variant = half ? 1 : 0;
@@ -614,6 +606,7 @@ static int build_eval(mmx_batch* b, std::vector<Launch>& out, int mode, bool com
       t.push_back(div_up(z.nrows, zrows_per_tile(g.first, 3)));
     }
     if ((rc = add_launch(b, out, L_ZINV, g.first, mode, a, t)) != MMX_OK) return rc;
+    out.back().inst = g.second;
     for (size_t k = 0; k < g.second.size(); k++)
       b->hext_off[g.second[k]].push_back(out.back().args_off + k * sizeof(ZinvArgs) + offsetof(ZinvArgs, ea) +
                                          offsetof(EpiArgs, lf) + offsetof(LocalField, hext));
@@ -625,7 +618,6 @@ static void batch_free(mmx_batch* b) {
   if (!b) return;
   if (b->gexec) cudaGraphExecDestroy(b->gexec);
   for (cudaStream_t q : b->par) cudaStreamDestroy(q);
-  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   for (cudaEvent_t e : b->ev_join) cudaEventDestroy(e);
   for (void* p : b->owned) cudaFree(p);
   if (b->owns)
@@ -736,6 +728,7 @@ static int batch_build(mmx_batch* b) {
       }
       rc = add_launch(b, b->finalize, L_FIN, 0, 0, a, t);
       if (rc == MMX_OK) {
+        for (int i = 0; i < (int)b->inst.size(); i++) b->finalize.back().inst.push_back(i);
         // clear the per-instance torque maxima before the step
         std::vector<float*> tq;
         for (mmx_solver* s : b->inst) tq.push_back(s->scratch + 1);
@@ -810,52 +803,85 @@ extern "C" mmx_solver* mmx_batch_instance(mmx_batch* b, int i) {
   return b->inst[i];
 }
 
-#define BATCH_MAX_PAR 8
-
-// Launches ls[0..n) of one pass on parallel branches forked from st and
-// joined back into it (used while st is being captured into a graph).
-static cudaError_t run_pass_parallel(mmx_batch* b, const Launch* ls, int n, cudaStream_t st) {
-  if (n == 1) return run_launch(ls[0], st);
+// While a step is captured into its graph, every launch depends only on the
+// latest earlier launch of each instance it touches (each instance's
+// buffers are its own), not on a whole pass: small instances run ahead
+// through their passes while large ones are still being transformed.
+// Launches are spread round-robin over BATCH_DAG_STREAMS streams; events
+// carry the per-instance dependencies.
+#define BATCH_DAG_STREAMS 16
+static cudaError_t batch_step_dag(mmx_batch* b, cudaStream_t st) {
   cudaError_t e;
-  while ((int)b->par.size() < BATCH_MAX_PAR) {
+  const int ninst = (int)b->inst.size();
+  size_t nl = 4 + b->finalize.size();
+  for (auto& stage : b->stage) nl += stage.size();
+  while ((int)b->par.size() < BATCH_DAG_STREAMS) {
     cudaStream_t q;
     if ((e = cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking)) != cudaSuccess) return e;
     b->par.push_back(q);
+  }
+  while (b->ev_join.size() < nl) {
     cudaEvent_t ev;
     if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
     b->ev_join.push_back(ev);
   }
-  if (!b->ev_fork && (e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming)) != cudaSuccess) return e;
-  const int P = n < BATCH_MAX_PAR ? n : BATCH_MAX_PAR;
-  if ((e = cudaEventRecord(b->ev_fork, st)) != cudaSuccess) return e;
-  for (int k = 0; k < P; k++)
-    if ((e = cudaStreamWaitEvent(b->par[k], b->ev_fork, 0)) != cudaSuccess) return e;
-  for (int i = 0; i < n; i++)
-    if ((e = run_launch(ls[i], b->par[i % P])) != cudaSuccess) return e;
-  for (int k = 0; k < P; k++) {
-    if ((e = cudaEventRecord(b->ev_join[k], b->par[k])) != cudaSuccess) return e;
-    if ((e = cudaStreamWaitEvent(st, b->ev_join[k], 0)) != cudaSuccess) return e;
+  size_t ne = 0;
+  // the origin: the torque maxima cleared on the capturing stream
+  if (b->torque_ptrs) {
+    kb_clear<<<(ninst + 255) / 256, 256, 0, st>>>(b->torque_ptrs, ninst);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
+  cudaEvent_t origin = b->ev_join[ne++];
+  if ((e = cudaEventRecord(origin, st)) != cudaSuccess) return e;
+  std::vector<cudaEvent_t> last(ninst, origin);
+  int rr = 0;
+  auto run = [&](const Launch& l) -> cudaError_t {
+    cudaStream_t q = b->par[rr++ % BATCH_DAG_STREAMS];
+    std::vector<cudaEvent_t> waits;
+    for (int i : l.inst) {
+      bool seen = false;
+      for (cudaEvent_t w : waits) seen = seen || w == last[i];
+      if (!seen) waits.push_back(last[i]);
+    }
+    cudaError_t r;
+    for (cudaEvent_t w : waits)
+      if ((r = cudaStreamWaitEvent(q, w, 0)) != cudaSuccess) return r;
+    if ((r = run_launch(l, q)) != cudaSuccess) return r;
+    cudaEvent_t done = b->ev_join[ne++];
+    if ((r = cudaEventRecord(done, q)) != cudaSuccess) return r;
+    for (int i : l.inst) last[i] = done;
+    return cudaSuccess;
+  };
+  for (auto& stage : b->stage)
+    for (const Launch& l : stage)
+      if ((e = run(l)) != cudaSuccess) return e;
+  for (const Launch& l : b->finalize)
+    if ((e = run(l)) != cudaSuccess) return e;
+  // join: the capturing stream waits for every instance's last launch
+  std::vector<cudaEvent_t> tails;
+  for (int i = 0; i < ninst; i++) {
+    bool seen = false;
+    for (cudaEvent_t w : tails) seen = seen || w == last[i];
+    if (!seen) tails.push_back(last[i]);
+  }
+  for (cudaEvent_t w : tails)
+    if ((e = cudaStreamWaitEvent(st, w, 0)) != cudaSuccess) return e;
   return cudaSuccess;
 }
 
 static cudaError_t batch_step_launches(mmx_batch* b, cudaStream_t st, bool parallel) {
+  if (parallel) return batch_step_dag(b, st);
   if (b->torque_ptrs) {
     int n = (int)b->inst.size();
     kb_clear<<<(n + 255) / 256, 256, 0, st>>>(b->torque_ptrs, n);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  for (auto& stage : b->stage) {
-    for (size_t i = 0; i < stage.size();) {
-      size_t j = i + 1;
-      if (parallel)
-        while (j < stage.size() && phase_of(stage[j]) == phase_of(stage[i])) j++;
-      cudaError_t e = run_pass_parallel(b, &stage[i], (int)(j - i), st);
+  for (auto& stage : b->stage)
+    for (const Launch& l : stage) {
+      cudaError_t e = run_launch(l, st);
       if (e != cudaSuccess) return e;
-      i = j;
     }
-  }
   for (const Launch& l : b->finalize) {
     cudaError_t e = run_launch(l, st);
     if (e != cudaSuccess) return e;

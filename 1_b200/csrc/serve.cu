@@ -14,8 +14,8 @@
 // chunk of check_every steps through one mmx_batch (one launch per pass and
 // line length, one CUDA graph per step), so requests that arrive while
 // others run join at the next chunk boundary and share the launches; when
-// at most two solves remain resident they step on their own solver graphs,
-// whose per-step latency is lower.  In plain mode the same loop runs
+// a single solve remains resident it steps on its own solver graph, whose
+// per-step latency is lower.  In plain mode the same loop runs
 // one solve at a time on the single-instance solver: the baseline the
 // batching is measured against.
 //
@@ -73,9 +73,10 @@ struct mmx_server {
 };
 
 // resident solves at or below which a batched server steps each solve on
-// its own graph (measured: two; with four, or with one stream per solve,
-// the served throughput was lower)
-static const int SOLO_MAX = 2;
+// its own graph (measured per step, RK4: one solve 0.129 ms alone vs 0.141
+// ms as a batch of one; two solves 0.238 ms one after the other vs 0.159 ms
+// batched)
+static const int SOLO_MAX = 1;
 
 static double sv_clock(const mmx_server* sv) {
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - sv->t0).count();

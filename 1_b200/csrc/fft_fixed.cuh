@@ -180,6 +180,35 @@ __device__ __forceinline__ void stage_rows(float2* s, const float2* tw, bool inv
   __syncthreads();
 }
 
+// A row-tile stage whose outputs past L/2 are never read (the last inverse
+// stage of a zero-padded line): only the lower half is computed and stored.
+template <int L, int R, int NS, int NLINES, int T, int PITCH>
+__device__ __forceinline__ void stage_rows_lower(float2* s, const float2* tw, bool inv) {
+  static_assert(NS * R == L, "the lower-half store is for the last stage");
+  using S = St<L, R, NS, NLINES, T, false>;
+  float2 v[S::NB][R];
+#pragma unroll
+  for (int i = 0; i < S::NB; i++) {
+    if (!S::valid(i)) continue;
+    int l, j;
+    S::lj(i, l, j);
+#pragma unroll
+    for (int q = 0; q < R; q++) v[i][q] = s[l * PITCH + padi(S::in_idx(j, q))];
+    S::twiddle(v[i], j, tw, inv);
+    dft<R>(v[i], inv);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < S::NB; i++) {
+    if (!S::valid(i)) continue;
+    int l, j;
+    S::lj(i, l, j);
+#pragma unroll
+    for (int q = 0; q < R / 2; q++) s[l * PITCH + padi(S::out_idx(j, q))] = v[i][q];
+  }
+  __syncthreads();
+}
+
 // stages [ST, ST1) of a forward or inverse transform of a row tile
 template <int L, int ST, int ST1, int NLINES, int T, int PITCH, bool INV>
 struct MidRows {

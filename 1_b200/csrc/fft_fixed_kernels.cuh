@@ -480,7 +480,17 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
     for (int q = 0; q < R0; q++) sm[l * PITCH + padi(S0::out_idx(j, q))] = v[q];
   }
   __syncthreads();
-  MidRows<M, 1, NST, NL, T, PITCH, true>::run(sm, tw);
+  if constexpr (NST >= 2) {
+    if (N2 == M) {
+      // open boundary: the cells use the lower half of each line only
+      MidRows<M, 1, NST - 1, NL, T, PITCH, true>::run(sm, tw);
+      stage_rows_lower<M, inv_radix(M, NST - 1), inv_span(M, NST - 1), NL, T, PITCH>(sm, tw, true);
+    } else {
+      MidRows<M, 1, NST, NL, T, PITCH, true>::run(sm, tw);
+    }
+  } else {
+    MidRows<M, 1, NST, NL, T, PITCH, true>::run(sm, tw);
+  }
   float lmax = 0.f;
   const int64_t g0 = (int64_t)r0 * N2;
   if (N2 == M) {

@@ -33,7 +33,6 @@ struct BCol {
   const float2* src;
   float2* dst;
   ColPass cp;
-  int ntx;  // column tiles per plane
 };
 struct BZr2c {
   const float* src;
@@ -53,7 +52,7 @@ __global__ void __launch_bounds__(T) kb_col(const BCol* __restrict__ a, const in
   int s = find_seg(starts, nseg, blockIdx.x);
   int t = blockIdx.x - starts[s];
   const BCol& c = a[s];
-  col_body<L, TK, T, INV, HALF>(c.src, c.dst, c.cp, t % c.ntx, t / c.ntx);
+  col_body<L, TK, T, INV, HALF>(c.src, c.dst, c.cp, t);
 }
 template <int L, int TK, int T, bool D2, bool HALF>
 __global__ void __launch_bounds__(T) kb_conv(const ConvArgs* __restrict__ a, const int* __restrict__ starts,
@@ -355,7 +354,7 @@ static int col_tiles(int L, int ncols, int nplanes, int variant) {
     FX_SIZES(C_)
 #undef C_
   }
-  return div_up(ncols, tk) * nplanes;
+  return div_up(ncols * nplanes, tk);
 }
 static int conv_tiles(int L, int ncols) {
   int tk = 1;
@@ -412,7 +411,6 @@ static void col_args(mmx_batch* b, int L, int inv, const std::vector<int>& ids, 
     c.cp.n_out = inv ? s->N[1] : s->P[1];
     c.cp.inv = inv;
     int tiles = col_tiles(L, c.cp.ncols, c.cp.nplanes, variant);
-    c.ntx = tiles / c.cp.nplanes;
     a.push_back(c);
     t.push_back(tiles);
   }

@@ -21,15 +21,25 @@ __host__ __device__ constexpr int odd_pitch(int lines) { return (lines % 2) ? li
 // HALF: forward, the input holds data in its lower half only (n_in = L/2);
 // inverse, only the lower half of the output is kept (n_out = L/2).
 template <int L, int TK, int T, bool INV, bool HALF>
-__device__ __forceinline__ void col_body(const float2* src, float2* dst, const ColPass& cp, int bx, int by) {
+__device__ __forceinline__ void col_body(const float2* src, float2* dst, const ColPass& cp, int tile) {
   __shared__ float2 tw[L];
   extern __shared__ float2 sm[];
   constexpr int NST = n_stages(L);
   constexpr int TKP = odd_pitch(TK);
   load_twiddles<L, T>(tw, cp.f.tw, cp.f.tws);
-  const int c0 = bx * TK;
-  const int64_t pbase = (int64_t)by * cp.plane_stride + c0;
-  const int nc = min(TK, cp.ncols - c0);
+  // Tiles run over the flattened columns of all planes: column g is column
+  // g % ncols of plane g / ncols, so a tile may straddle two planes and no
+  // tile at the end of a plane is left mostly empty.
+  const int nall = cp.nplanes * cp.ncols;
+  auto col_at = [&](int l, int64_t& base) -> bool {
+    const int g = tile * TK + l;
+    const int pl = g / cp.ncols;
+    base = (int64_t)pl * cp.plane_stride + (g - pl * cp.ncols);
+    return g < nall;
+  };
+  // T % TK == 0: every butterfly of a thread is in the same column
+  int64_t base0;
+  const bool ok0 = col_at((int)threadIdx.x % TK, base0);
   const int64_t sti = cp.stride_i;
   const int n_in = cp.n_in, n_out = cp.n_out;
   constexpr int R0 = INV ? inv_radix(L, 0) : fwd_radix(L, 0);
@@ -40,10 +50,13 @@ __device__ __forceinline__ void col_body(const float2* src, float2* dst, const C
     if (!S0::valid(i)) continue;
     int l, j;
     S0::lj(i, l, j);
+    int64_t cbase = base0;
+    bool ok = ok0;
+    if constexpr (T % TK != 0) ok = col_at(l, cbase);
 #pragma unroll
     for (int q = 0; q < R0; q++) {
       int idx = S0::in_idx(j, q);
-      v[i][q] = (((HALF && !INV) ? q < R0 / 2 : idx < n_in) && l < nc) ? src[pbase + idx * sti + l]
+      v[i][q] = (((HALF && !INV) ? q < R0 / 2 : idx < n_in) && ok) ? src[cbase + idx * sti]
                                                                         : make_float2(0.f, 0.f);
     }
     if (HALF && !INV) dft_half<R0>(v[i], INV);
@@ -55,10 +68,13 @@ __device__ __forceinline__ void col_body(const float2* src, float2* dst, const C
       if (!S0::valid(i)) continue;
       int l, j;
       S0::lj(i, l, j);
+      int64_t cbase = base0;
+      bool ok = ok0;
+      if constexpr (T % TK != 0) ok = col_at(l, cbase);
 #pragma unroll
       for (int q = 0; q < R0; q++) {
         int idx = S0::out_idx(j, q);
-        if (((HALF && INV) ? q < R0 / 2 : idx < n_out) && l < nc) dst[pbase + idx * sti + l] = v[i][q];
+        if (((HALF && INV) ? q < R0 / 2 : idx < n_out) && ok) dst[cbase + idx * sti] = v[i][q];
       }
     }
   } else {
@@ -81,6 +97,9 @@ __device__ __forceinline__ void col_body(const float2* src, float2* dst, const C
       if (!SL::valid(i)) continue;
       int l, j;
       SL::lj(i, l, j);
+      int64_t cbase = base0;
+      bool ok = ok0;
+      if constexpr (T % TK != 0) ok = col_at(l, cbase);
 #pragma unroll
       for (int q = 0; q < RL; q++) w[i][q] = sm[SL::in_idx(j, q) * TKP + l];
       SL::twiddle(w[i], j, tw, INV);
@@ -88,7 +107,7 @@ __device__ __forceinline__ void col_body(const float2* src, float2* dst, const C
 #pragma unroll
       for (int q = 0; q < RL; q++) {
         int idx = SL::out_idx(j, q);
-        if (((HALF && INV) ? q < RL / 2 : idx < n_out) && l < nc) dst[pbase + idx * sti + l] = w[i][q];
+        if (((HALF && INV) ? q < RL / 2 : idx < n_out) && ok) dst[cbase + idx * sti] = w[i][q];
       }
     }
   }
@@ -96,7 +115,7 @@ __device__ __forceinline__ void col_body(const float2* src, float2* dst, const C
 
 template <int L, int TK, int T, bool INV, bool HALF>
 __global__ void __launch_bounds__(T) k_col_fx(const float2* src, float2* dst, ColPass cp) {
-  col_body<L, TK, T, INV, HALF>(src, dst, cp, blockIdx.x, blockIdx.y);
+  col_body<L, TK, T, INV, HALF>(src, dst, cp, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------
@@ -630,7 +649,7 @@ cudaError_t fx_launch_col(const float2* src, float2* dst, const ColPass& cp, cud
   constexpr int TK = fx_col_tk(L);
   constexpr int T = fx_threads(TK * L);
   size_t smem = sizeof(float2) * (size_t)odd_pitch(TK) * L;
-  dim3 grid(div_up(cp.ncols, TK), cp.nplanes);
+  const int grid = div_up(cp.ncols * cp.nplanes, TK);
   const bool half = 2 * (INV ? cp.n_out : cp.n_in) == L;
   if (half) {
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_col_fx<L, TK, T, INV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

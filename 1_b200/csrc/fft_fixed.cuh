@@ -87,6 +87,17 @@ struct St {
       v[q] = inv ? cmulc_f(v[q], w) : cmul_f(v[q], w);
     }
   }
+  // the same, from a table in [q][k] order: tw[q * NS + k] = W^(q k TSTEP)
+  __device__ __forceinline__ static void twiddle_qk(float2* v, int j, const float2* tw, bool inv) {
+    static_assert(NS * R == L, "a [q][k] table holds the last stage's twiddles");
+    if (NS == 1) return;
+    int k = j % NS;
+#pragma unroll
+    for (int q = 1; q < R; q++) {
+      float2 w = tw[q * NS + k];
+      v[q] = inv ? cmulc_f(v[q], w) : cmul_f(v[q], w);
+    }
+  }
 };
 
 template <int R>
@@ -154,7 +165,27 @@ __host__ __device__ constexpr int row_pitch(int L) {
 }
 __device__ __forceinline__ int padi(int i) { return i + (i >> 4); }
 
-template <int L, int R, int NS, int NLINES, int T, int PITCH>
+// Row tiles map butterflies j-fastest, so the lanes of a half-warp read the
+// twiddles tw[q k] for consecutive k: entries q apart, a gcd(q, 16)-way bank
+// conflict for even q.  When the only stage with twiddles is the second of
+// two equal-radix stages (256 = 16 * 16, 64 = 8 * 8; the same stage shape in
+// the forward and the inverse transform), the table is kept in [q][k] order
+// instead (QK) and a half-warp reads consecutive entries.
+template <int L>
+__host__ __device__ constexpr bool rows_qk() {
+  return n_stages(L) == 2 && fwd_radix(L, 0) == fwd_radix(L, 1);
+}
+template <int L, int T>
+__device__ __forceinline__ void load_twiddles_rows(float2* tw, const float2* __restrict__ g, int gstride) {
+  if constexpr (rows_qk<L>()) {
+    constexpr int R = fwd_radix(L, 0);
+    for (int e = threadIdx.x; e < L; e += T) tw[e] = __ldg(&g[(e / R) * (e % R) * gstride]);
+  } else {
+    load_twiddles<L, T>(tw, g, gstride);
+  }
+}
+
+template <int L, int R, int NS, int NLINES, int T, int PITCH, bool QK = false>
 __device__ __forceinline__ void stage_rows(float2* s, const float2* tw, bool inv) {
   using S = St<L, R, NS, NLINES, T, false>;
   float2 v[S::NB][R];
@@ -165,7 +196,8 @@ __device__ __forceinline__ void stage_rows(float2* s, const float2* tw, bool inv
     S::lj(i, l, j);
 #pragma unroll
     for (int q = 0; q < R; q++) v[i][q] = s[l * PITCH + padi(S::in_idx(j, q))];
-    S::twiddle(v[i], j, tw, inv);
+    if constexpr (QK) S::twiddle_qk(v[i], j, tw, inv);
+    else S::twiddle(v[i], j, tw, inv);
     dft<R>(v[i], inv);
   }
   __syncthreads();
@@ -182,7 +214,7 @@ __device__ __forceinline__ void stage_rows(float2* s, const float2* tw, bool inv
 
 // A row-tile stage whose outputs past L/2 are never read (the last inverse
 // stage of a zero-padded line): only the lower half is computed and stored.
-template <int L, int R, int NS, int NLINES, int T, int PITCH>
+template <int L, int R, int NS, int NLINES, int T, int PITCH, bool QK = false>
 __device__ __forceinline__ void stage_rows_lower(float2* s, const float2* tw, bool inv) {
   static_assert(NS * R == L, "the lower-half store is for the last stage");
   using S = St<L, R, NS, NLINES, T, false>;
@@ -194,7 +226,8 @@ __device__ __forceinline__ void stage_rows_lower(float2* s, const float2* tw, bo
     S::lj(i, l, j);
 #pragma unroll
     for (int q = 0; q < R; q++) v[i][q] = s[l * PITCH + padi(S::in_idx(j, q))];
-    S::twiddle(v[i], j, tw, inv);
+    if constexpr (QK) S::twiddle_qk(v[i], j, tw, inv);
+    else S::twiddle(v[i], j, tw, inv);
     dft<R>(v[i], inv);
   }
   __syncthreads();
@@ -210,14 +243,14 @@ __device__ __forceinline__ void stage_rows_lower(float2* s, const float2* tw, bo
 }
 
 // stages [ST, ST1) of a forward or inverse transform of a row tile
-template <int L, int ST, int ST1, int NLINES, int T, int PITCH, bool INV>
+template <int L, int ST, int ST1, int NLINES, int T, int PITCH, bool INV, bool QK = false>
 struct MidRows {
   __device__ __forceinline__ static void run(float2* s, const float2* tw) {
     if constexpr (ST < ST1) {
       constexpr int R = INV ? inv_radix(L, ST) : fwd_radix(L, ST);
       constexpr int NS = INV ? inv_span(L, ST) : fwd_span(L, ST);
-      stage_rows<L, R, NS, NLINES, T, PITCH>(s, tw, INV);
-      MidRows<L, ST + 1, ST1, NLINES, T, PITCH, INV>::run(s, tw);
+      stage_rows<L, R, NS, NLINES, T, PITCH, QK>(s, tw, INV);
+      MidRows<L, ST + 1, ST1, NLINES, T, PITCH, INV, QK>::run(s, tw);
     }
   }
 };

@@ -325,7 +325,8 @@ __device__ __forceinline__ void zr2c_body(const float* __restrict__ src, float2*
   extern __shared__ float2 sm[];
   constexpr int PITCH = row_pitch(M);
   constexpr int NST = n_stages(M);
-  load_twiddles<M, T>(tw, z.f.tw, z.f.tws);
+  constexpr bool QK = rows_qk<M>();
+  load_twiddles_rows<M, T>(tw, z.f.tw, z.f.tws);
   const int r0 = bx * RT;
   const int nl = min(RT, z.nrows - r0);
   if (threadIdx.x < RT) {
@@ -375,7 +376,7 @@ __device__ __forceinline__ void zr2c_body(const float* __restrict__ src, float2*
     for (int q = 0; q < R0; q++) sm[l * PITCH + padi(S0::out_idx(j, q))] = v[q];
   }
   __syncthreads();
-  MidRows<M, 1, NST, RT, T, PITCH, false>::run(sm, tw);
+  MidRows<M, 1, NST, RT, T, PITCH, false, QK>::run(sm, tw);
   for (int e = threadIdx.x; e < nl * (M + 1); e += T) {
     int l = e / (M + 1), k = e - l * (M + 1);
     float2 Zk = sm[l * PITCH + padi(k == M ? 0 : k)];
@@ -467,7 +468,8 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
   const int P1 = za.P1, HZ = za.HZ, nrows = za.nrows;
   const int64_t CS = za.CS;
   const EpiArgs& ea = za.ea;
-  load_twiddles<M, T>(tw, za.twz, 2);
+  constexpr bool QK = rows_qk<M>();
+  load_twiddles_rows<M, T>(tw, za.twz, 2);
   const int r0 = bx * RT;
   const int nr = min(RT, nrows - r0);
   const int N1 = ea.N1, N2 = ea.N2;
@@ -502,13 +504,13 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
   if constexpr (NST >= 2) {
     if (N2 == M) {
       // open boundary: the cells use the lower half of each line only
-      MidRows<M, 1, NST - 1, NL, T, PITCH, true>::run(sm, tw);
-      stage_rows_lower<M, inv_radix(M, NST - 1), inv_span(M, NST - 1), NL, T, PITCH>(sm, tw, true);
+      MidRows<M, 1, NST - 1, NL, T, PITCH, true, QK>::run(sm, tw);
+      stage_rows_lower<M, inv_radix(M, NST - 1), inv_span(M, NST - 1), NL, T, PITCH, QK>(sm, tw, true);
     } else {
-      MidRows<M, 1, NST, NL, T, PITCH, true>::run(sm, tw);
+      MidRows<M, 1, NST, NL, T, PITCH, true, QK>::run(sm, tw);
     }
   } else {
-    MidRows<M, 1, NST, NL, T, PITCH, true>::run(sm, tw);
+    MidRows<M, 1, NST, NL, T, PITCH, true, QK>::run(sm, tw);
   }
   float lmax = 0.f;
   const int64_t g0 = (int64_t)r0 * N2;
@@ -572,7 +574,7 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
         for (int q = 0; q < F0; q++) sm[l * PITCH + padi(SF::out_idx(j, q))] = f[i][q];
       }
       __syncthreads();
-      MidRows<M, 1, NST, NL, T, PITCH, false>::run(sm, tw);
+      MidRows<M, 1, NST, NL, T, PITCH, false, QK>::run(sm, tw);
       for (int e = threadIdx.x; e < 3 * nr * (M + 1); e += T) {
         int l = e / (M + 1), k = e - l * (M + 1);
         int r = l / 3, c = l - 3 * r;

@@ -107,6 +107,30 @@ def test_fused_steps_vs_oracle(eng, cuda, solver, steps):
     assert abs(st["time"] - o.time()) <= 1e-6 * abs(o.time())
 
 
+@pytest.mark.parametrize("grid", [(64, 8, 2), (256, 4, 2)])
+def test_fused_heun_two_stage_z_vs_oracle(eng, cuda, grid):
+    """Z lines of two equal-radix stages (the user's x = 64 -> 8 x 8 and
+    256 -> 16 x 16 complex points after the real-to-complex packing) keep
+    their twiddles in [q][k] order in the Z passes: the field and 10 fused
+    Heun steps still match the FP64 oracle."""
+    c = anis_cube_like(grid)
+    kw = dict(solver="heun", dt=1e-14)
+    m = O.seeded_m(grid, 6, "random")
+    o = O.OracleSim(O.make_cfg(**c, **kw), m, bits=64)
+    s = eng.Solver(eng.mmx_params(**c, **kw))
+    mm = o.m().astype(np.float32)
+    dm = cuda.from_numpy(mm.copy()).cuda()
+    dh = cuda.zeros_like(dm)
+    s.field(P(dm), P(dh))
+    cuda.cuda.synchronize()
+    h64 = o.heff(mm.astype(np.float64))
+    assert np.abs(dh.cpu().numpy() - h64).max() / np.abs(h64).max() < 2e-6
+    s.set_m(mm)
+    o.steps(10)
+    s.step(10)
+    assert np.abs(s.get_m() - o.m()).max() < 1e-5
+
+
 def test_fused_vs_primitive_heun(eng, cuda):
     """Fused Heun (mmx_solver_step) and the drop-in primitive sequence the Go
     driver issues agree to rounding."""

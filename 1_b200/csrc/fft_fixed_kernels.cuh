@@ -377,17 +377,19 @@ __device__ __forceinline__ void zr2c_body(const float* __restrict__ src, float2*
   }
   __syncthreads();
   MidRows<M, 1, NST, RT, T, PITCH, false, QK>::run(sm, tw);
-  for (int e = threadIdx.x; e < nl * (M + 1); e += T) {
-    int l = e / (M + 1), k = e - l * (M + 1);
-    float2 Zk = sm[l * PITCH + padi(k == M ? 0 : k)];
+  // R2C split, one thread per pair (k, M - k), k <= M/2:
+  // X_k = E_k + w^k O_k and X_{M-k} = conj(E_k - w^k O_k)
+  constexpr int HP = M / 2 + 1;
+  for (int e = threadIdx.x; e < nl * HP; e += T) {
+    int l = e / HP, k = e - l * HP;
+    float2 Zk = sm[l * PITCH + padi(k)];
     float2 Zm = sm[l * PITCH + padi(k == 0 ? 0 : M - k)];
     float2 E = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
     float2 O = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
-    float2 w = tw[0];
-    if (k == M) w = make_float2(-1.f, 0.f);
-    else w = __ldg(&z.twP[k]);
-    float2 wo = cmul_f(w, O);
-    dst[soff_s[l] + k] = make_float2(E.x + wo.x, E.y + wo.y);
+    float2 wo = cmul_f(__ldg(&z.twP[k]), O);
+    float2* row = dst + soff_s[l];
+    row[k] = make_float2(E.x + wo.x, E.y + wo.y);
+    if (k < M / 2) row[M - k] = make_float2(E.x - wo.x, wo.y - E.y);
   }
 }
 
@@ -575,16 +577,20 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
       }
       __syncthreads();
       MidRows<M, 1, NST, NL, T, PITCH, false, QK>::run(sm, tw);
-      for (int e = threadIdx.x; e < 3 * nr * (M + 1); e += T) {
-        int l = e / (M + 1), k = e - l * (M + 1);
+      // R2C split, one thread per pair (k, M - k), k <= M/2:
+      // X_k = E_k + w^k O_k and X_{M-k} = conj(E_k - w^k O_k)
+      constexpr int HP = M / 2 + 1;
+      for (int e = threadIdx.x; e < 3 * nr * HP; e += T) {
+        int l = e / HP, k = e - l * HP;
         int r = l / 3, c = l - 3 * r;
-        float2 Zk = sm[l * PITCH + padi(k == M ? 0 : k)];
+        float2 Zk = sm[l * PITCH + padi(k)];
         float2 Zm = sm[l * PITCH + padi(k == 0 ? 0 : M - k)];
         float2 E = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
         float2 O = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
-        float2 w = (k == M) ? make_float2(-1.f, 0.f) : __ldg(&twP[k]);
-        float2 wo = cmul_f(w, O);
-        za.S[c * CS + rbase_s[r] + k] = make_float2(E.x + wo.x, E.y + wo.y);
+        float2 wo = cmul_f(__ldg(&twP[k]), O);
+        float2* row = za.S + c * CS + rbase_s[r];
+        row[k] = make_float2(E.x + wo.x, E.y + wo.y);
+        if (k < M / 2) row[M - k] = make_float2(E.x - wo.x, wo.y - E.y);
       }
       return;
     }

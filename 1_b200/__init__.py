@@ -223,6 +223,9 @@ MMX = {
                                         ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
                                         ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_longlong)]),
     "mmx_solver_set_hext": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "mmx_solver_energy": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    "mmx_solver_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_float, ctypes.c_void_p, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_int), ctypes.c_longlong, ctypes.c_void_p]),
     "mmx_solver_m_device": (ctypes.c_void_p, [ctypes.c_void_p]),
     "mmx_solver_use_graph": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "mmx_solver_device_control": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -280,6 +283,10 @@ DRIVER = {
     "mmxd_dt": (ctypes.c_float, [ctypes.c_void_p]),
     "mmxd_torque": (ctypes.c_float, [ctypes.c_void_p]),
     "mmxd_step_count": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "mmxd_step_error": (ctypes.c_float, [ctypes.c_void_p]),
+    "mmxd_energy": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "mmxd_run_table": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_float, ctypes.c_void_p, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_int)]),
 }
 
 _cache = {}
@@ -430,6 +437,22 @@ class Solver:
         _check(lib().mmx_solver_state(self.h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(tq), ctypes.byref(er),
                                       ctypes.byref(st)))
         return dict(time=t.value, dt=dt.value, torque=tq.value, error=er.value, steps=st.value)
+
+    def energy(self, stream=None):
+        """Total energy of m, internal units (mmx_solver_energy)."""
+        e = ctypes.c_double()
+        _check(lib().mmx_solver_energy(self.h, ctypes.byref(e), stream))
+        return e.value
+
+    def run(self, seconds, period, max_rows=100000, max_steps=0, stream=None):
+        """Sim.Run for 'seconds' with a table row every 'period' seconds:
+        returns an (nrows, 7) array {t, <m> (user x,y,z), torque, min m_z,
+        max m_z} (mmx_solver_run)."""
+        rows = np.zeros((max(max_rows, 1), 7), np.float32)
+        n = ctypes.c_int()
+        _check(lib().mmx_solver_run(self.h, seconds, period, rows.ctypes.data, max_rows, ctypes.byref(n), max_steps,
+                                    stream))
+        return rows[:n.value]
 
     def m_device(self):
         return lib().mmx_solver_m_device(self.h)
@@ -864,3 +887,28 @@ class DriverSim:
 
     def torque(self):
         return driver().mmxd_torque(self.h)
+
+    def step_error(self):
+        return driver().mmxd_step_error(self.h)
+
+    def steps_taken(self):
+        return driver().mmxd_step_count(self.h)
+
+    def energy(self, m=None):
+        """Total energy (internal units) of m (default: the current m)."""
+        a = np.ascontiguousarray(self.m() if m is None else m, dtype=np.float32)
+        e = ctypes.c_float()
+        rc = driver().mmxd_energy(self.h, a.ctypes.data, ctypes.byref(e))
+        if rc:
+            raise MmxError(driver().mmxd_last_error().decode())
+        return e.value
+
+    def run_table(self, seconds, period, max_rows=100000):
+        """Sim.Run with a table row every 'period' seconds (7 floats per
+        row, as Solver.run)."""
+        rows = np.zeros((max(max_rows, 1), 7), np.float32)
+        n = ctypes.c_int()
+        rc = driver().mmxd_run_table(self.h, seconds, period, rows.ctypes.data, max_rows, ctypes.byref(n))
+        if rc:
+            raise MmxError(driver().mmxd_last_error().decode())
+        return rows[:n.value]

@@ -38,6 +38,8 @@ struct mmxd_lib {
   void (*normalize)(float*, int);
   void (*deltaM)(float*, float*, float, float*, float, int);
   void (*local)(float*, float*, int, float*, float*, int, float*, float*);
+  void (*local_phi)(float*, float*, float*, int, float*, float*, int, float*, float*);
+  void (*scale_dot)(float*, float*, float*, float, int);
   void (*kmul6)(float*, float*, float*, float*, float*, float*, float*, float*, float*, int);
   void (*kmul4)(float*, float*, float*, float*, float*, float*, float*, int);
   void* (*plan_new)(int*, int*);
@@ -70,6 +72,8 @@ extern "C" mmxd_lib* mmxd_open(const char* path) {
             sym(h, "gpu_madd", &L->madd) && sym(h, "gpu_linear_combination", &L->lincomb) &&
             sym(h, "gpu_reduce", &L->reduce) && sym(h, "gpu_normalize_uniform", &L->normalize) &&
             sym(h, "gpu_deltaM", &L->deltaM) && sym(h, "gpu_add_local_fields", &L->local) &&
+            sym(h, "gpu_add_local_fields_H_and_phi", &L->local_phi) &&
+            sym(h, "gpu_scale_dot_product", &L->scale_dot) &&
             sym(h, "gpu_kernelmul6", &L->kmul6) && sym(h, "gpu_kernelmul4", &L->kmul4) &&
             sym(h, "new_gpuFFT3dPlan_padded", &L->plan_new) && sym(h, "delete_gpuFFT3dPlan", &L->plan_del) &&
             sym(h, "gpuFFT3dPlan_forward", &L->fwd) && sym(h, "gpuFFT3dPlan_inverse", &L->inv);
@@ -106,7 +110,7 @@ struct Reductor {
   float reduce(mmxd_lib* L, float* in) { return L->reduce(op, in, dev, host.data(), blocks, threads, N); }
 };
 
-enum { RED_ADD = 1, RED_MAXABS = 3 };
+enum { RED_ADD = 1, RED_MAX = 2, RED_MAXABS = 3, RED_MIN = 4 };
 
 struct mmxd_sim {
   mmxd_lib* L;
@@ -132,8 +136,10 @@ struct mmxd_sim {
   float a[7][7], b[7], b2[7], c[7];
   float* k[7] = {nullptr};
   float *m0 = nullptr, *mbackup = nullptr, *m1est = nullptr, *t0 = nullptr;
-  Reductor maxabs, sum;
+  Reductor maxabs, sum, vmin, vmax;
   float avgNorm = 1;
+  float* phi = nullptr;     // energy density (initEDens, energy.go:71-78)
+  float since = 0;          // Periodic.sinceoutput of the table (simoutput.go:77-80)
   std::vector<float*> owned;
 };
 
@@ -257,6 +263,8 @@ extern "C" mmxd_sim* mmxd_new(mmxd_lib* L, const mmxd_config* cfg, const float* 
   L->memcpy_dir((float*)m_init, s->m, s->n3, 1);
   s->maxabs.init(L, RED_MAXABS, s->n3);
   s->sum.init(L, RED_ADD, s->n);
+  s->vmin.init(L, RED_MIN, s->n);
+  s->vmax.init(L, RED_MAX, s->n);
   // convolution (init.go:234-274, conv.go:35-167)
   s->ktype = s->P[0] == 1 ? 4 : 6;
   int complexN = s->P[0] * s->P[1] * (s->P[2] + 2);
@@ -310,6 +318,9 @@ extern "C" void mmxd_free(mmxd_sim* s) {
   for (float* p : s->owned) s->L->free_array(p);
   if (s->maxabs.dev) s->L->free_array(s->maxabs.dev);
   if (s->sum.dev) s->L->free_array(s->sum.dev);
+  if (s->vmin.dev) s->L->free_array(s->vmin.dev);
+  if (s->vmax.dev) s->L->free_array(s->vmax.dev);
+  if (s->phi) s->L->free_array(s->phi);
   if (s->plan) s->L->plan_del(s->plan);
   delete s;
 }
@@ -461,6 +472,67 @@ extern "C" int mmxd_avg_m(mmxd_sim* s, float out[3]) {
   for (int c = 0; c < 3; c++) out[c] = f_div(s->sum.reduce(s->L, s->m + (int64_t)c * s->n), s->avgNorm);
   return MMX_OK;
 }
+// Total energy of m (host array), internal units: calcHeffEnergy
+// (field.go:64-71,83-87) -- the demag + exchange field, phi = -1/2 m.h
+// (ScaledDotProduct, field.go:17-20), the local fields and their energy
+// density (AddLocalFieldsEdens, field.go:44-47), sumEdens (energy.go:49-52):
+// the Reductor's sum of phi times the cell volume (energy.go:38-44).
+extern "C" int mmxd_energy(mmxd_sim* s, const float* m, float* out) {
+  mmxd_lib* L = s->L;
+  if (!s->phi) s->phi = L->new_array(s->n);
+  float* dm = alloc3(s);
+  float* dh = alloc3(s);
+  L->memcpy_dir((float*)m, dm, s->n3, 1);
+  convolve(s, dm, dh);
+  L->scale_dot(s->phi, dm, dh, -0.5f, s->n);
+  float K[3] = {s->anisK[0], s->anisK[1], s->anisK[2]};
+  L->local_phi(dm, dh, s->phi, s->n, s->hext, nullptr, s->anis, K, s->axes);
+  float total = s->sum.reduce(L, s->phi);
+  float vol = f_mul(f_mul(s->cs[0], s->cs[1]), s->cs[2]);
+  *out = f_mul(total, vol);
+  L->free_array(dm);
+  L->free_array(dh);
+  s->owned.pop_back();
+  s->owned.pop_back();
+  return MMX_OK;
+}
+
+// Sim.Run with a periodic table output (simrun.go:19-57; Periodic.NeedSave
+// simoutput.go:83-85; Table.Save simoutput.go:226-272): before each step,
+// with t = float32(time) * UnitTime, a row is written when t == 0 or
+// t - sinceoutput >= period: {t, <m> in user order (the Reductor's sums /
+// N), the last maximum torque, min and max of internal component X (the
+// user's m_z)}, then sinceoutput = t.  *nrows = rows written (<= max_rows).
+extern "C" int mmxd_run_table(mmxd_sim* s, double seconds, float period, float* rows, int max_rows, int* nrows) {
+  mmxd_lib* L = s->L;
+  double stop = s->time + seconds / (double)s->unitT;
+  L->normalize(s->m, s->n);
+  int k = 0;
+  while (s->time < stop) {
+    float t = f_mul((float)s->time, s->unitT);
+    volatile float d = t - s->since;
+    if ((t == 0.f || d >= period) && k < max_rows) {
+      float* r = rows + 7 * k;
+      float av[3];
+      mmxd_avg_m(s, av);
+      r[0] = t;
+      r[1] = av[2];
+      r[2] = av[1];
+      r[3] = av[0];
+      r[4] = s->torque;
+      r[5] = s->vmin.reduce(L, s->m);
+      r[6] = s->vmax.reduce(L, s->m);
+      s->since = t;
+      k++;
+    }
+    int rc = step(s);
+    if (rc) { *nrows = k; return rc; }
+  }
+  *nrows = k;
+  return MMX_OK;
+}
+
+extern "C" float mmxd_step_error(mmxd_sim* s) { return s->stepError; }
 extern "C" double mmxd_time(mmxd_sim* s) { return s->time; }
 extern "C" float mmxd_dt(mmxd_sim* s) { return s->dt; }
 extern "C" float mmxd_torque(mmxd_sim* s) { return s->torque; }

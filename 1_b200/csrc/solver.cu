@@ -846,6 +846,7 @@ extern "C" int mmx_face_kernel6(const int P[3], const int periodic[3], const flo
 
 static void solver_free(mmx_solver* s) {
   if (!s) return;
+  solver_run_free(s);
   if (s->gexec) cudaGraphExecDestroy(s->gexec);
   for (int g = 0; g < 2; g++)
     if (s->dgraph[g]) cudaGraphExecDestroy(s->dgraph[g]);
@@ -1009,6 +1010,20 @@ extern "C" int mmx_solver_field(mmx_solver* s, const float* m, float* h, cudaStr
   return MMX_OK;
 }
 
+int solver_field_conv(mmx_solver* s, const float* m, float* h, cudaStream_t st) {
+  s->spec_ready = 0;
+  cudaError_t e = conv_front(s, m, st);
+  if (e == cudaSuccess) {
+    EpiArgs ea = solver_base_args(s);
+    memset(&ea.lf, 0, sizeof(ea.lf));  // h + 0: the convolution alone
+    ea.m_in = m;
+    ea.out0 = h;
+    e = launch_zinv<EPI_FIELD>(s, ea, st);
+  }
+  if (e != cudaSuccess) { mmx_set_error(cudaGetErrorString(e)); return MMX_ERR_CUDA; }
+  return MMX_OK;
+}
+
 static int step_once(mmx_solver* s, cudaStream_t st) {
   if (s->p.solver == MMX_SOLVER_HEUN) {
     cudaError_t e = heun_step(s, st);
@@ -1032,15 +1047,6 @@ static int step_once(mmx_solver* s, cudaStream_t st) {
 // untouched; the next replay retries with the reduced dt.  No host
 // synchronisation per step.
 // ---------------------------------------------------------------------
-struct RkDev {
-  double time;
-  float dt;
-  int accept;
-  long long accepted, trials;
-  float torque, err;
-  int bad;
-};
-
 __global__ void k_fsal_copy(float* __restrict__ k0, const float* __restrict__ klast, int64_t n3,
                             const RkDev* __restrict__ dev, int faithful, float* __restrict__ torque) {
   const bool copy = dev->accept || faithful;  // rk.go:311-315 (retry: faithful reuses the rejected k_last)
@@ -1159,6 +1165,9 @@ static int rk_device_download(mmx_solver* s) {
   s->trials = h.trials;
   return MMX_OK;
 }
+
+cudaError_t solver_device_trial(mmx_solver* s, cudaStream_t st, bool first) { return rk_device_trial(s, st, first); }
+int solver_device_download(mmx_solver* s) { return rk_device_download(s); }
 
 extern "C" int mmx_solver_device_control(mmx_solver* s, int on) {
   if (!s) { mmx_set_error("null argument"); return MMX_ERR_ARG; }

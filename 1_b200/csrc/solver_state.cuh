@@ -16,6 +16,16 @@ struct PassTimer {
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
 };
 
+// Device-side state of the adaptive RK controller (mmx_solver_device_control).
+struct RkDev {
+  double time;
+  float dt;
+  int accept;
+  long long accepted, trials;
+  float torque, err;
+  int bad;
+};
+
 struct mmx_solver {
   mmx_params p;
   int N[3], P[3], HZ;
@@ -54,6 +64,14 @@ struct mmx_solver {
   int use_graph = 0;
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t gstream = nullptr;
+  // run loop with table output (run.cu)
+  void* runbuf = nullptr;                 // RunDev on the device
+  float* rows_dev = nullptr;              // device table rows
+  int rows_cap = 0;
+  float since = 0.f;                      // Periodic.sinceoutput (seconds, float32)
+  cudaGraphExec_t rungraph = nullptr;     // devctl: WHILE-conditional run graph
+  cudaStream_t rungraph_stream = nullptr;
+  double* eacc = nullptr;                 // energy accumulator (one double)
   // profiling
   int profile = 0;
   std::vector<PassTimer> timers;
@@ -69,3 +87,12 @@ static inline float f32_add(float a, float b) { volatile float r = a + b; return
 EpiArgs solver_base_args(mmx_solver* s);
 // Device launch grid for a 1D element-wise kernel over n items.
 int solver_grid_1d(int64_t n);
+// h = demag + exchange field of the device array m (no local fields).
+int solver_field_conv(mmx_solver* s, const float* m, float* h, cudaStream_t st);
+// One trial of the device-controlled adaptive RK step (first: no FSAL
+// value yet), as plain launches on st (capturable).
+cudaError_t solver_device_trial(mmx_solver* s, cudaStream_t st, bool first);
+// Reads the device controller's time, dt and step counts back (syncs).
+int solver_device_download(mmx_solver* s);
+// Frees the run loop's buffers and graph (run.cu).
+void solver_run_free(mmx_solver* s);

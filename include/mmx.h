@@ -100,6 +100,33 @@ int mmx_solver_field(mmx_solver* s, const float* m, float* h, cudaStream_t strea
  * pointer. */
 int mmx_solver_avg_m(mmx_solver* s, float* out3, int on_host, cudaStream_t stream);
 
+/* Total energy of the resident m in internal units (multiply by the
+ * energy unit A*L, material.go:51-111, for joules): what the reference
+ * computes with calcHeffEnergy + sumEdens (src/go/sim/field.go:64-71,
+ * energy.go:38-52) -- phi = -1/2 m.h_demag+exch - m.Hext - 1/2 K (m.u)^2 per
+ * cell (gpu_linalg.cu:125-140, gpu_local_contr3.cu:230-247,362-374), summed
+ * in float64 on the device, times the cell volume.  Synchronous; uses one
+ * field evaluation. */
+int mmx_solver_energy(mmx_solver* s, double* energy, cudaStream_t stream);
+
+/* Sim.Run with the periodic table output (src/go/sim/simrun.go:19-57,
+ * simoutput.go:76-90,226-272): normalises m, then steps while the time is
+ * below time + seconds / UnitTime.  Before each step, when
+ * t = float32(time) * UnitTime (seconds) is 0 or at least 'period' past the
+ * last row, one row of 7 floats is reduced on the device:
+ *   {t, <m_x>, <m_y>, <m_z> (user axes), last maximum torque (0 for heun),
+ *    min m_z, max m_z (the user's z = internal X component)}
+ * At most max_rows rows are copied to the host array 'rows'; *nrows gets
+ * their count; successive calls continue the output schedule.  Fixed-step
+ * and host-controlled solvers step from the host (no read-back except the
+ * adaptive controller's own); with mmx_solver_device_control the whole run
+ * is one CUDA graph launch (a WHILE conditional node over {row check, one
+ * RK trial, loop condition}) with no host synchronisation until it ends.
+ * max_steps > 0 caps the steps (device controller: 16 x max_steps trials;
+ * MMX_ERR_STATE if the cap ends the run early); 0 = no cap.  Synchronous. */
+int mmx_solver_run(mmx_solver* s, double seconds, float period, float* rows, int max_rows, int* nrows,
+                   long long max_steps, cudaStream_t stream);
+
 /* Solver scalars: simulated time (internal units), current dt, the last
  * maximum torque and the last error estimate, steps taken. */
 int mmx_solver_state(mmx_solver* s, double* time, float* dt, float* max_torque, float* step_error, long long* steps);

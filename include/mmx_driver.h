@@ -71,6 +71,16 @@ double mmxd_time(mmxd_sim* s);                /* internal units */
 float mmxd_dt(mmxd_sim* s);                   /* internal units */
 float mmxd_torque(mmxd_sim* s);               /* last maximum torque */
 long long mmxd_step_count(mmxd_sim* s);
+float mmxd_step_error(mmxd_sim* s);           /* last error estimate of an adaptive step */
+/* Total energy of m (host, internal layout) in internal units:
+ * calcHeffEnergy + sumEdens (field.go:64-71, energy.go:49-52). */
+int mmxd_energy(mmxd_sim* s, const float* m, float* out);
+/* Sim.Run for 'seconds' with a table row every 'period' seconds
+ * (simrun.go:19-57, simoutput.go:83-85,226-272); 7 floats per row:
+ * t (s), <m> (user x,y,z), last maximum torque, min and max of the user's
+ * m_z.  *nrows = rows written, at most max_rows.  Successive calls continue
+ * the output schedule. */
+int mmxd_run_table(mmxd_sim* s, double seconds, float period, float* rows, int max_rows, int* nrows);
 
 #ifdef __cplusplus
 }

@@ -158,6 +158,37 @@ class OracleSim:
         rt = ctypes.c_float if self.bits == 32 else ctypes.c_double
         return _fn(self.bits, "sim_torque", rt)(ctypes.c_void_p(self.h))
 
+    def energy(self, m=None):
+        """Total energy (internal units) of m (default: the current m):
+        calcHeffEnergy + sumEdens (field.go:64-71, energy.go:49-52)."""
+        m = self.m() if m is None else np.ascontiguousarray(m, dtype=_dt(self.bits))
+        out = np.zeros(1, _dt(self.bits))
+        f = _fn(self.bits, "sim_energy")
+        f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        f(ctypes.c_void_p(self.h), _ptr(m), _ptr(out))
+        return float(out[0])
+
+    def run_table(self, seconds, period, max_rows=100000):
+        """Sim.Run for 'seconds' (SI) with a table row every 'period'
+        seconds (simrun.go:19-57, simoutput.go:83-85,226-272).  Rows:
+        t (s), <m> (user x, y, z), last maximum torque, min and max of the
+        user's m_z.  Successive calls continue the schedule."""
+        if not hasattr(self, "_since"):
+            self._since = np.zeros(1, np.float32)
+        rows = np.zeros((max_rows, 7), np.float32)
+        f = _fn(self.bits, "sim_run_table", ctypes.c_int)
+        f.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_float, ctypes.c_void_p, ctypes.c_int,
+                      ctypes.c_void_p]
+        k = f(ctypes.c_void_p(self.h), seconds / self.unit("time"), period, _ptr(rows), max_rows,
+              _ptr(self._since))
+        if k < 0:
+            raise RuntimeError("oracle: dt is NaN")
+        return rows[:k]
+
+    def step_error(self):
+        rt = ctypes.c_float if self.bits == 32 else ctypes.c_double
+        return _fn(self.bits, "sim_step_error", rt)(ctypes.c_void_p(self.h))
+
 
 def face_kernel6(P, cs, periodic=(0, 0, 0), accuracy=8, bits=32):
     dt = _dt(bits)
@@ -235,6 +266,33 @@ def add_local_fields(m, h, hext, anis=0, K=0.0, u=(0, 0, 0), bits=32):
                   ctypes.c_float if bits == 32 else ctypes.c_double, ctypes.c_void_p]
     f(_ptr(m), _ptr(h), m.size // 3, _ptr(he), anis, K, _ptr(ua))
     return h
+
+
+def scale_dot_product(a, b, sc, bits=32):
+    """phi = sc (a . b) per cell of two [3][N] arrays (gpu_linalg.cu:125-140)."""
+    dt = _dt(bits)
+    a = np.ascontiguousarray(a, dtype=dt)
+    b = np.ascontiguousarray(b, dtype=dt)
+    n = a.size // 3
+    phi = np.empty(n, dt)
+    f = _fn(bits, "scale_dot_product")
+    f.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_float if bits == 32 else ctypes.c_double, ctypes.c_int64]
+    f(_ptr(phi), _ptr(a), _ptr(b), sc, n)
+    return phi
+
+
+def add_local_fields_phi(m, h, phi, hext, anis=0, K=0.0, u=(0, 0, 0), bits=32):
+    """gpu_add_local_fields_H_and_phi (uniform field): returns (h', phi')."""
+    dt = _dt(bits)
+    m = np.ascontiguousarray(m, dtype=dt)
+    h = np.array(h, dtype=dt, copy=True)
+    phi = np.array(phi, dtype=dt, copy=True)
+    n = m.size // 3
+    f = _fn(bits, "add_local_fields_phi")
+    f.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_float if bits == 32 else ctypes.c_double, ctypes.c_void_p]
+    f(_ptr(m), _ptr(h), _ptr(phi), n, _ptr(np.asarray(hext, dt)), anis, K, _ptr(np.asarray(u, dt)))
+    return h, phi
 
 
 def ref_sum(a, maxthreads=1024, bits=32):

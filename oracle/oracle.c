@@ -453,6 +453,44 @@ void FN(add_local_fields)(const REAL* m, REAL* h, int64_t N, const REAL hext[3],
   }
 }
 
+/* gpu_scale_dot_product (gpu_linalg.cu:125-140):
+ * phi_i = s (a_x b_x + a_y b_y + a_z b_z), left to right. */
+void FN(scale_dot_product)(REAL* phi, const REAL* a, const REAL* b, REAL sc, int64_t N) {
+#pragma omp parallel for
+  for (int64_t i = 0; i < N; i++) {
+    REAL d = a[i] * b[i];
+    d = d + a[N + i] * b[N + i];
+    d = d + a[2 * N + i] * b[2 * N + i];
+    phi[i] = sc * d;
+  }
+}
+
+/* gpu_add_local_fields_H_and_phi, uniform Hext, ANIS_NONE and
+ * ANIS_UNIAXIAL (gpu_local_contr3.cu:230-247,362-374,395-466): the fields
+ * of add_local_fields, and
+ *   phi -= m.Hext + ((0.5 K) mu) (m.u)
+ * with each dot product summed left to right. */
+void FN(add_local_fields_phi)(const REAL* m, REAL* h, REAL* phi, int64_t N, const REAL hext[3], int anis, REAL K,
+                              const REAL u[3]) {
+  FN(add_local_fields)(m, h, N, hext, anis, K, u);
+#pragma omp parallel for
+  for (int64_t i = 0; i < N; i++) {
+    REAL mh = m[i] * hext[0];
+    mh = mh + m[N + i] * hext[1];
+    mh = mh + m[2 * N + i] * hext[2];
+    if (anis != 0) {
+      REAL mu = m[i] * u[0];
+      mu = mu + m[N + i] * u[1];
+      mu = mu + m[2 * N + i] * u[2];
+      REAL t = (REAL)0.5 * K;
+      t = t * mu;
+      t = t * mu;
+      mh = mh + t;
+    }
+    phi[i] = phi[i] - mh;
+  }
+}
+
 /* gpu_deltaM (gpu_torque.cu:20-54): h <- dt_gilb (m x h + alpha m x (m x h))
  * in the internal (left-handed) frame. */
 void FN(delta_m)(const REAL* m, REAL* h, int64_t N, REAL alpha, REAL dtg) {
@@ -900,6 +938,80 @@ void FN(sim_avg_m)(void* p, REAL out[3]) {
   osim_t* s = (osim_t*)p;
   for (int c = 0; c < 3; c++) out[c] = FN(ref_sum)(s->m + c * s->n, s->n, s->cfg.maxthreads) / (REAL)s->n;
 }
+/* Total energy of m, internal units: calcHeffEnergy (field.go:64-71,
+ * 83-87): the demag + exchange field h, phi = -1/2 m.h
+ * (calcHDemagExchEdens, field.go:17-20), the local fields and their energy
+ * density (addLocalFieldsEdens, field.go:44-47), then sumEdens
+ * (energy.go:49-52): the Reductor's sum of phi times the cell volume
+ * cs_X cs_Y cs_Z (energy.go:38-44).  The FP32 build sums in the
+ * reference's partial-sum order; the FP64 build sums in float64. */
+void FN(sim_energy)(void* p, const REAL* m, REAL* out) {
+  osim_t* s = (osim_t*)p;
+  REAL* h = (REAL*)malloc(sizeof(REAL) * 3 * s->n);
+  REAL* phi = (REAL*)malloc(sizeof(REAL) * s->n);
+  convolve(&s->conv, m, h);
+  FN(scale_dot_product)(phi, m, h, (REAL)-0.5, s->n);
+  FN(add_local_fields_phi)(m, h, phi, s->n, s->hext, s->cfg.anis, s->K, s->u);
+  REAL total;
+  if (sizeof(REAL) == 4) {
+    total = FN(ref_sum)(phi, s->n, s->cfg.maxthreads);
+  } else {
+    double acc = 0;
+    for (int64_t i = 0; i < s->n; i++) acc += (double)phi[i];
+    total = (REAL)acc;
+  }
+  REAL vol = s->cs[0] * s->cs[1];
+  vol = vol * s->cs[2];
+  *out = total * vol;
+  free(h);
+  free(phi);
+}
+
+/* Sim.Run with a periodic table output (simrun.go:19-57,
+ * simoutput.go:76-90,226-272): before each step, Periodic.NeedSave with
+ * the float32 time t = float32(time) * UnitTime (t == 0 or
+ * t - sinceoutput >= period) writes one row
+ *   {t, <m_x>, <m_y>, <m_z>, torque, min m_z, max m_z}
+ * in user order (<m_x> is the internal Z component; <m> is the Reductor's
+ * sum / N, simoutput.go:236-239; torque is the last maximum torque,
+ * simoutput.go:250-257; min/max of internal component X,
+ * simoutput.go:258-261), then sinceoutput = t.  Steps while
+ * time < stop (internal units).  Returns the rows written (at most
+ * max_rows) or -1 on a NaN; *since carries sinceoutput between calls. */
+int FN(sim_run_table)(void* p, double duration, float period, float* rows, int max_rows, float* since) {
+  osim_t* s = (osim_t*)p;
+  double stop = s->time + duration;
+  int nrow = 0;
+  FN(normalize)(s->m, s->n);
+  while (s->time < stop) {
+    float t = (float)s->time;
+    volatile float tt = t * (float)s->T;
+    t = tt;
+    volatile float d = t - *since;
+    if ((t == 0.f || d >= period) && nrow < max_rows) {
+      float* r = rows + 7 * nrow;
+      REAL av[3];
+      FN(sim_avg_m)(p, av);
+      r[0] = t;
+      r[1] = (float)av[2];
+      r[2] = (float)av[1];
+      r[3] = (float)av[0];
+      r[4] = (float)s->torque;
+      REAL mn = s->m[0], mx = s->m[0];
+      for (int64_t i = 1; i < s->n; i++) {
+        if (s->m[i] < mn) mn = s->m[i];
+        if (s->m[i] > mx) mx = s->m[i];
+      }
+      r[5] = (float)mn;
+      r[6] = (float)mx;
+      *since = t;
+      nrow++;
+    }
+    if (FN(sim_step)(p)) return -1;
+  }
+  return nrow;
+}
+
 REAL FN(sim_torque)(void* p) { return ((osim_t*)p)->torque; }
 REAL FN(sim_step_error)(void* p) { return ((osim_t*)p)->step_error; }
 

@@ -156,3 +156,45 @@ def test_driver_exports():
     txt = open(os.path.join(ROOT, "include", "mmx_driver.h")).read()
     for name in re.findall(r"\b(mmxd_\w+)\s*\(", txt):
         assert name in exported, name
+
+
+def test_energy_zeeman_and_anisotropy_terms():
+    """Energy of a uniform state: switching on a field adds -N (m.B) V and a
+    uniaxial term adds -1/2 K (m.u)^2 N V (gpu_local_contr3.cu:230-247,
+    362-374, energy.go:38-52), in both oracle builds."""
+    base = dict(grid=(16, 8, 2), cell=(5e-9, 5e-9, 5e-9), msat=8e5, aexch=1.3e-11, alpha=0.1)
+    m = np.zeros((3, 2, 8, 16), np.float32)
+    m[2] = 1.0  # internal Z = the user's x
+    for bits in (32, 64):
+        e0 = O.OracleSim(O.make_cfg(**base), m, bits=bits)
+        eb = O.OracleSim(O.make_cfg(**base, bext=(0.05, 0.0, 0.0)), m, bits=bits)
+        ek = O.OracleSim(O.make_cfg(**base, anis=1, k1=4e5, axis=(1, 0, 0)), m, bits=bits)
+        cs = e0.internal_params()["cellsize"]
+        vol = float(cs[0]) * float(cs[1]) * float(cs[2])
+        n = 16 * 8 * 2
+        hx = 0.05 / e0.unit("field")
+        dz = eb.energy() - e0.energy()
+        assert abs(dz - (-n * hx * vol)) <= 2e-5 * abs(n * hx * vol)
+        K = ek.internal_params()["K"]
+        da = ek.energy() - e0.energy()
+        assert abs(da - (-0.5 * float(K) * n * vol)) <= 2e-5 * abs(0.5 * float(K) * n * vol)
+        # demag self-energy of the uniform state is positive
+        assert e0.energy() > 0
+
+
+def test_run_table_schedule():
+    """Sim.Run's table: the first row at t = 0, each later row at the first
+    step boundary at or past 'period' after the previous one; a second call
+    continues the schedule."""
+    c = dict(grid=(32, 8, 1), cell=(3.90625e-9, 3.90625e-9, 3e-9), msat=8e5, aexch=1.3e-11, alpha=0.02,
+             bext=(-24.6e-3, 4.3e-3, 0.0), solver="rk23", maxerror=1e-5)
+    o = O.OracleSim(O.make_cfg(**c), O.seeded_m(c["grid"], 1, "tilted"), bits=32)
+    r1 = o.run_table(3e-11, 1e-11)
+    r2 = o.run_table(3e-11, 1e-11)
+    r = np.concatenate([r1, r2])
+    assert r[0, 0] == 0 and len(r) == 6
+    gaps = np.diff(r[:, 0])
+    assert np.all(gaps >= np.float32(1e-11) * (1 - 1e-6))
+    assert np.all(gaps <= 1e-11 + 2 * o.dt() * o.unit("time"))
+    assert np.allclose(np.linalg.norm(r[:, 1:4], axis=1) <= 1.0 + 1e-6, True)
+    assert np.all(r[:, 5] <= r[:, 6])

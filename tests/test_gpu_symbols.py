@@ -1,0 +1,490 @@
+"""Symbol-by-symbol parity of the drop-in libgpukern exports with the
+reference's own library (src/gpukern built from its sources for sm_100a into
+oracle/_ref/libgpukern_ref.so) on identical inputs.
+
+The reference library is compiled with --use_fast_math (common.mk:22-33):
+products may be contracted into FMAs and rsqrtf / __expf / __sinf replace
+the correctly rounded functions, so element-wise results are compared within
+a stated number of float32 ulps (or an absolute bound relative to the data
+where terms cancel); pure data movement is compared for equality.  Every
+size below was checked against the reference kernels' index arithmetic
+(grid shapes and bounds checks) before use."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import REF_LIB
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference library not built here")]
+
+
+def P(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def ints(*v):
+    return (ctypes.c_int * len(v))(*v)
+
+
+def fa(*v):
+    return (ctypes.c_float * len(v))(*[float(x) for x in v])
+
+
+@pytest.fixture(scope="module")
+def libs(eng, cuda):
+    mine = eng.lib()
+    mine.gpu_init(0, 0)
+    ref = ctypes.CDLL(REF_LIB)
+    for name, (res, args) in eng.ABI.items():
+        f = getattr(ref, name, None)
+        if f is not None:
+            f.restype = res
+            f.argtypes = args
+    ref.gpu_init(0, 0)
+    return mine, ref
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).cuda()
+
+
+def both(torch, libs, fn, *arrays):
+    """Runs fn(lib, device copies of arrays) for both libraries and returns
+    the host copies of the arrays after each call."""
+    out = []
+    for lib in libs:
+        ds = [dev(torch, a) for a in arrays]
+        fn(lib, ds)
+        torch.cuda.synchronize()
+        out.append([d.cpu().numpy() for d in ds])
+    return out
+
+
+def ulp_dev(a, b):
+    a = np.asarray(a, np.float32).ravel()
+    b = np.asarray(b, np.float32).ravel()
+    ia = a.view(np.int32).astype(np.int64)
+    ib = b.view(np.int32).astype(np.int64)
+    ia = np.where(ia < 0, -(ia & 0x7fffffff), ia)
+    ib = np.where(ib < 0, -(ib & 0x7fffffff), ib)
+    return int(np.abs(ia - ib).max()) if a.size else 0
+
+
+def close(a, b, ulps=4, rel=1e-6):
+    """Within 'ulps' of each other, or within rel x max|b| (cancellation)."""
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    if ulp_dev(a, b) <= ulps:
+        return True
+    return bool(np.abs(a.astype(np.float64) - b).max() <= rel * max(np.abs(b).max(), 1e-30))
+
+
+def rnd(shape, seed, scale=1.0):
+    return (np.random.default_rng(seed).standard_normal(shape) * scale).astype(np.float32)
+
+
+# ---------------------------------------------------------------- algebra
+def test_add_madd_madd2_add_constant_lincomb(libs, cuda):
+    n = 10007
+    a, b, c = rnd(n, 1), rnd(n, 2), rnd(n, 3)
+
+    def run(L, d):
+        L.gpu_add(P(d[0]), P(d[1]), n)
+        L.gpu_madd(P(d[0]), ctypes.c_float(0.37), P(d[1]), n)
+        L.gpu_madd2(P(d[0]), P(d[1]), P(d[2]), n)
+        L.gpu_add_constant(P(d[0]), ctypes.c_float(-1.25), n)
+        L.gpu_linear_combination(P(d[0]), P(d[2]), ctypes.c_float(0.5), ctypes.c_float(-2.0), n)
+
+    (x,), (y,) = [[o[0]] for o in both(cuda, libs, run, a, b, c)]
+    assert close(x, y, ulps=2)
+
+
+def test_linear_combination_many(libs, cuda):
+    """The reference kernel reads result[i] before its bounds check
+    (gpu_linalg.cu:103-108): n is a multiple of its 1024-thread blocks and
+    the result buffer carries one more block, so every read is in bounds."""
+    n, nv = 4096, 3
+    r = rnd(n + 1024, 4)
+    vs = [rnd(n, 5 + i) for i in range(nv)]
+    w = np.array([0.25, -1.5, 3.0], np.float32)
+    outs = []
+    for L in libs:
+        dr = dev(cuda, r)
+        dv = [dev(cuda, v) for v in vs]
+        ptrs = cuda.tensor([t.data_ptr() for t in dv], dtype=cuda.int64, device="cuda")
+        dw = dev(cuda, w)
+        L.gpu_linear_combination_many(P(dr), P(ptrs), P(dw), nv, n)
+        cuda.cuda.synchronize()
+        outs.append(dr.cpu().numpy()[:n])
+    assert close(outs[0], outs[1], ulps=4)
+
+
+def test_scale_dot_product(libs, cuda):
+    n = 5003
+    a, b = rnd((3, n), 7), rnd((3, n), 8)
+    res = np.zeros(n, np.float32)
+
+    def run(L, d):
+        L.gpu_scale_dot_product(P(d[2]), P(d[0]), P(d[1]), ctypes.c_float(-0.5), n)
+
+    o1, o2 = both(cuda, libs, run, a, b, res)
+    assert close(o1[2], o2[2], ulps=4, rel=1e-6)
+
+
+# --------------------------------------------------------- normalise, torque
+def test_normalize_uniform_and_map(libs, cuda):
+    n = 6007
+    m = rnd((3, n), 9, 1.7)
+    mp = np.abs(rnd(n, 10)) + 0.5
+    mp[::17] = 0.0
+
+    def run(L, d):
+        L.gpu_normalize_uniform(P(d[0]), n)
+        L.gpu_normalize_map(P(d[1]), P(d[2]), n)
+
+    o1, o2 = both(cuda, libs, run, m, m, mp)
+    assert close(o1[0], o2[0], ulps=4)  # reference: rsqrtf (fast math), here correctly rounded
+    assert close(o1[1], o2[1], ulps=4)
+    assert np.all(o1[1][:, ::17] == 0) and np.all(o2[1][:, ::17] == 0)
+
+
+def test_deltaM_with_alpha_map(libs, cuda):
+    n = 4097
+    m = O.normalize(rnd((3, n), 11))
+    h = rnd((3, n), 12, 2.0)
+    amap = np.abs(rnd(n, 13)) + 0.1
+
+    def run(L, d):
+        L.gpu_deltaM(P(d[0]), P(d[1]), ctypes.c_float(0.3), P(d[2]), ctypes.c_float(0.01), n)
+
+    o1, o2 = both(cuda, libs, run, m, h, amap)
+    assert close(o1[1], o2[1], ulps=8, rel=2e-6)
+
+
+# ------------------------------------------------------------ local fields
+@pytest.mark.parametrize("anis", [0, 1, 2])
+@pytest.mark.parametrize("hmap", [False, True])
+def test_add_local_fields(libs, cuda, anis, hmap):
+    if anis == 2 and hmap:
+        # the reference reads Hext[Y*N] from the 3-float host array here
+        # (gpu_local_contr3.cu:217): undefined, so not run
+        pytest.skip("reference reads past its host field array for cubic anisotropy with a field map")
+    n = 3001
+    m = O.normalize(rnd((3, n), 14))
+    h = rnd((3, n), 15)
+    hm = rnd((3, n), 16) if hmap else np.zeros((3, 1), np.float32)
+    K = fa(0.7, -0.2, 0)
+    if anis == 2:
+        ax = fa(1, 0, 0, 0, 0.6, 0.8, 0, -0.8, 0.6)
+    else:
+        ax = fa(0.0, 0.6, 0.8)
+
+    def run(L, d):
+        L.gpu_add_local_fields(P(d[0]), P(d[1]), n, fa(0.02, -0.01, 0.005), P(d[2]) if hmap else None, anis, K, ax)
+
+    o1, o2 = both(cuda, libs, run, m, h, hm)
+    assert close(o1[1], o2[1], ulps=4, rel=1e-6)
+
+
+@pytest.mark.parametrize("anis", [0, 1, 2])
+def test_add_local_fields_H_and_phi(libs, cuda, anis):
+    n = 3001
+    m = O.normalize(rnd((3, n), 17))
+    h = rnd((3, n), 18)
+    phi = rnd(n, 19)
+    K = fa(0.7, -0.2, 0)
+    ax = fa(1, 0, 0, 0, 0.6, 0.8, 0, -0.8, 0.6) if anis == 2 else fa(0.0, 0.6, 0.8)
+
+    def run(L, d):
+        L.gpu_add_local_fields_H_and_phi(P(d[0]), P(d[1]), P(d[2]), n, fa(0.02, -0.01, 0.005), None, anis, K, ax)
+
+    o1, o2 = both(cuda, libs, run, m, h, phi)
+    assert close(o1[1], o2[1], ulps=4, rel=1e-6)
+    assert close(o1[2], o2[2], ulps=4, rel=1e-6)
+
+
+# --------------------------------------------------------------- exchange
+@pytest.mark.parametrize("size,per,typ", [
+    ((1, 20, 36), (0, 0, 0), 6), ((1, 20, 36), (0, 1, 1), 6),
+    ((6, 10, 18), (0, 0, 0), 6), ((6, 10, 18), (1, 0, 1), 6),
+    ((1, 20, 36), (0, 0, 0), 12), ((1, 20, 36), (0, 1, 1), 12),
+    ((6, 10, 18), (0, 0, 0), 12), ((6, 10, 18), (1, 1, 0), 12),
+])
+def test_add_exch(libs, cuda, size, per, typ):
+    n = size[0] * size[1] * size[2]
+    m = O.normalize(rnd((3, n), 20))
+    h = rnd((3, n), 21)
+    cs = fa(0.9, 0.7, 1.1)
+
+    def run(L, d):
+        L.gpu_add_exch(P(d[0]), P(d[1]), ints(*size), ints(*per), ints(0, 0, 0), cs, typ)
+
+    o1, o2 = both(cuda, libs, run, m, h)
+    a, b = o1[1], o2[1]
+    if typ == 6 and size[0] > 1 and per[0]:
+        # the reference's 3D six-neighbour kernel reads plane 1, not plane 0,
+        # as the periodic +X neighbour of the last plane (gpu_exch1.cu:164-
+        # 165: indg_in has already advanced one plane when it subtracts
+        # (Nx-1) planes); this library wraps to plane 0.  Compare every other
+        # plane with the reference, and the last plane with the stencil.
+        S = size[1] * size[2]
+        assert close(a.reshape(3, size[0], S)[:, :-1], b.reshape(3, size[0], S)[:, :-1], ulps=16, rel=2e-6)
+        want = laplacian(m, h, size, per, (0.9, 0.7, 1.1))
+        assert np.abs(a - want).max() <= 2e-6 * np.abs(want).max()
+        return
+    assert close(a, b, ulps=16, rel=2e-6)
+
+
+def laplacian(m, h, size, per, cs):
+    """h + the six-neighbour Laplacian of m (float64), open or periodic."""
+    M = m.astype(np.float64).reshape((3,) + tuple(size))
+    out = h.astype(np.float64).reshape((3,) + tuple(size)).copy()
+    for ax in range(3):
+        if size[ax] == 1:
+            continue
+        for sgn in (1, -1):
+            nb = np.roll(M, -sgn, axis=ax + 1)
+            if not per[ax]:
+                idx = [slice(None)] * 4
+                idx[ax + 1] = -1 if sgn == 1 else 0
+                nb[tuple(idx)] = 0.0
+            out += (nb - M) / cs[ax] ** 2
+    return out.reshape(h.shape)
+
+
+# -------------------------------------------------- other torque terms
+def test_spintorque_deltaM(libs, cuda):
+    N = (4, 12, 20)
+    n = N[0] * N[1] * N[2]
+    m = O.normalize(rnd((3, n), 22))
+    h = rnd((3, n), 23)
+    jm = np.abs(rnd((3, n), 24)) + 0.5
+    for use_map in (False, True):
+        def run(L, d):
+            L.gpu_spintorque_deltaM(P(d[0]), P(d[1]), ctypes.c_float(0.02), ctypes.c_float(0.04),
+                                    ctypes.c_float(0.7), fa(0.3, -0.2, 0.1), P(d[2]) if use_map else None,
+                                    ctypes.c_float(0.01), *N)
+
+        o1, o2 = both(cuda, libs, run, m, h, jm)
+        assert close(o1[1], o2[1], ulps=16, rel=2e-6)
+
+
+def test_anal_fw_step(libs, cuda):
+    n = 4001
+    m = O.normalize(rnd((3, n), 25))
+    h = rnd((3, n), 26, 0.5)
+    h[:2, ::50] = 0.0  # the h_x = h_y = 0 branch
+    out = np.zeros_like(m)
+
+    def run(L, d):
+        L.gpu_anal_fw_step(ctypes.c_float(0.05), ctypes.c_float(0.1), n, P(d[0]), P(d[2]), P(d[1]))
+
+    o1, o2 = both(cuda, libs, run, m, h, out)
+    # the reference uses __expf / __sincosf (fast math): compare to 2e-6
+    assert np.abs(o1[2] - o2[2]).max() <= 2e-6
+
+
+def test_lin_anisotropy(libs, cuda):
+    """The reference's host function is empty (gpu_anis.cu:44-50): its
+    kernel's arithmetic (gpu_anis.cu:19-40) is checked against numpy in
+    float64, and the reference call is checked to leave h unchanged."""
+    mine, ref = libs
+    n = 3001
+    m = O.normalize(rnd((3, n), 27))
+    h = rnd((3, n), 28)
+    k = rnd((6, n), 29)
+    dm, dh, dk = dev(cuda, m), dev(cuda, h), dev(cuda, k)
+    args = [P(dh[0]), P(dh[1]), P(dh[2]), P(dm[0]), P(dm[1]), P(dm[2])] + [P(dk[i]) for i in range(6)]
+    mine.gpu_add_lin_anisotropy(*args, n)
+    cuda.cuda.synchronize()
+    kxx, kyy, kzz, kyz, kxz, kxy = k.astype(np.float64)
+    M = m.astype(np.float64)
+    want = h.astype(np.float64) + np.stack([M[0] * kxx + M[1] * kxy + M[2] * kxz,
+                                            M[0] * kxy + M[1] * kyy + M[2] * kyz,
+                                            M[0] * kxz + M[1] * kyz + M[2] * kzz])
+    assert np.abs(dh.cpu().numpy() - want).max() <= 4e-6 * np.abs(want).max()
+    dh2 = dev(cuda, h)
+    args[0:3] = [P(dh2[0]), P(dh2[1]), P(dh2[2])]
+    ref.gpu_add_lin_anisotropy(*args, n)
+    cuda.cuda.synchronize()
+    assert np.array_equal(dh2.cpu().numpy(), h)
+
+
+# ----------------------------------------------------------- data movement
+@pytest.mark.parametrize("shape", [(4, 6, 16), (3, 32, 34), (1, 20, 48)])
+def test_transposes(libs, cuda, shape):
+    N0, N1, N2 = shape
+    a = rnd(N0 * N1 * N2, 30)
+    out = np.zeros_like(a)
+
+    def run_yz(L, d):
+        L.gpu_transpose_complex_YZ(P(d[0]), P(d[1]), N1, N2, N0)
+
+    def run_xz(L, d):
+        L.gpu_transpose_complex_XZ(P(d[0]), P(d[1]), N0, N1, N2)
+
+    for fn in (run_yz, run_xz):
+        o1, o2 = both(cuda, libs, fn, a, out)
+        assert np.array_equal(o1[1], o2[1])
+
+
+@pytest.mark.parametrize("S,D", [((3, 5, 7), (6, 10, 14)), ((1, 16, 9), (1, 32, 18)), ((2, 3, 4), (2, 3, 4))])
+def test_copy_pad_unpad(libs, cuda, S, D):
+    src = rnd(int(np.prod(S)), 31)
+    dst = rnd(int(np.prod(D)), 32)
+
+    def pad(L, d):
+        L.gpu_copy_pad(P(d[0]), P(d[1]), *S, *D)
+
+    o1, o2 = both(cuda, libs, pad, src, dst)
+    assert np.array_equal(o1[1], o2[1])
+    # unpad D -> S: the reference writes (D0 - S0) planes past its
+    # destination (gpu_zeropad.cu:97-107), so both get a guard region
+    big = rnd(int(np.prod(D)), 33)
+    guard = np.zeros(int(np.prod(S)) + (D[0] - S[0]) * S[1] * S[2], np.float32)
+
+    def unpad(L, d):
+        L.gpu_copy_unpad(P(d[0]), P(d[1]), *D, *S)
+
+    o1, o2 = both(cuda, libs, unpad, big, guard)
+    k = int(np.prod(S))
+    assert np.array_equal(o1[1][:k], o2[1][:k])
+
+
+def test_copy_pad2D_unpad2D(libs, cuda):
+    S, D = (12, 20), (24, 40)
+    src = rnd(S[0] * S[1], 34)
+    dst = rnd(D[0] * D[1], 35)
+
+    def pad(L, d):
+        L.gpu_copy_pad2D(P(d[0]), P(d[1]), *S, *D)
+
+    o1, o2 = both(cuda, libs, pad, src, dst)
+    assert np.array_equal(o1[1], o2[1])
+
+    def unpad(L, d):
+        L.gpu_copy_unpad2D(P(d[1]), P(d[0]), *D, *S)
+
+    o1, o2 = both(cuda, libs, unpad, src, dst)
+    assert np.array_equal(o1[0], o2[0])
+
+
+# ------------------------------------------------------- kernel products
+def test_kernelmul6_kernelmul4(libs, cuda):
+    nreal = 2 * 3000
+    mx, my, mz = rnd(nreal, 36), rnd(nreal, 37), rnd(nreal, 38)
+    ks = [rnd(nreal // 2, 40 + i) for i in range(6)]
+
+    def k6(L, d):
+        L.gpu_kernelmul6(*[P(x) for x in d], nreal)
+
+    def k4(L, d):
+        L.gpu_kernelmul4(*[P(x) for x in d[:7]], nreal)
+
+    for fn in (k6, k4):
+        o1, o2 = both(cuda, libs, fn, mx, my, mz, *ks)
+        for c in range(3):
+            assert close(o1[c], o2[c], ulps=4, rel=1e-6)
+
+
+# ------------------------------------------------------------- reductions
+@pytest.mark.parametrize("n", [2, 33, 1000, 4096, 20000, 262144])
+def test_gpu_reduce_all_ops(libs, eng, cuda, n):
+    """gpu_reduce with the Reductor's launch shape (redux.go:103-121).  MAX,
+    MIN, MAXABS are exact; the sums accumulate in float64 here and in the
+    reference's float32 tree, so they agree to the float32 rounding of
+    the sum's terms."""
+    mine, ref = libs
+    a = rnd(n, 50)
+    threads = mine.gpu_maxthreads() // 2
+    while n <= threads:
+        threads //= 2
+    blocks = (n - 1) // (threads * 2) + 1
+    d = dev(cuda, a)
+    for op in (1, 2, 3, 4, 5):
+        vals = []
+        for L in libs:
+            d2 = cuda.zeros(blocks, device="cuda")
+            h2 = np.zeros(blocks, np.float32)
+            vals.append(L.gpu_reduce(op, P(d), P(d2), h2.ctypes.data, blocks, threads, n))
+        exact = {1: a.astype(np.float64).sum(), 2: a.max(), 3: np.abs(a).max(), 4: a.min(),
+                 5: np.abs(a).astype(np.float64).sum()}[op]
+        if op in (2, 3, 4):
+            assert vals[0] == vals[1] == np.float32(exact), (op, vals, exact)
+        else:
+            bound = 1e-6 * np.abs(a).astype(np.float64).sum()
+            assert abs(vals[0] - exact) <= bound and abs(vals[1] - exact) <= 4 * bound, (op, vals, exact)
+
+
+# ---------------------------------------------------------------- transforms
+@pytest.mark.parametrize("N,Pd", [((1, 16, 32), (1, 32, 64)), ((4, 12, 20), (8, 24, 40)), ((3, 5, 14), (6, 10, 28))])
+def test_fft_plan_forward_inverse(libs, cuda, N, Pd):
+    """gpuFFT3dPlan_forward / _inverse of this library (own transforms)
+    against the reference's (cuFFT) on the same padded input: spectra within
+    1e-5 of the largest bin, the unnormalised round trip within 1e-5 of the
+    largest value (fft_test.go:160,224 allow 1e-4)."""
+    n = int(np.prod(N))
+    a = rnd(n, 60)
+    nspec = Pd[0] * Pd[1] * (Pd[2] + 2)
+    outs = []
+    for L in libs:
+        plan = L.new_gpuFFT3dPlan_padded(ints(*N), ints(*Pd))
+        din = dev(cuda, a)
+        spec = cuda.zeros(nspec, device="cuda")
+        back = cuda.zeros(n + (Pd[0] - N[0]) * N[1] * N[2], device="cuda")
+        L.gpuFFT3dPlan_forward(plan, P(din), P(spec))
+        s = spec.cpu().numpy()
+        L.gpuFFT3dPlan_inverse(plan, P(spec), P(back))
+        cuda.cuda.synchronize()
+        outs.append((s, back.cpu().numpy()[:n], L.gpuFFT3dPlan_normalization(plan)))
+        L.delete_gpuFFT3dPlan(plan)
+    (s1, b1, n1), (s2, b2, n2) = outs
+    assert n1 == n2
+    assert np.abs(s1 - s2).max() <= 1e-5 * np.abs(s2).max()
+    assert np.abs(b1 - b2).max() <= 1e-5 * np.abs(b2).max()
+    assert np.abs(b1 / n1 - a).max() <= 1e-5 * np.abs(a).max()
+
+
+# ------------------------------------------------------------ noise, memory
+def test_gaussian_noise_statistics(libs, cuda):
+    """gpu_gaussian_noise: the reference draws from cuRAND, this library from
+    Philox-4x32-10 + Box-Muller; both must give the requested mean and
+    standard deviation, fresh numbers per call and no correlation between
+    neighbours."""
+    n = 1 << 20
+    for L in libs:
+        d = cuda.zeros(n, device="cuda")
+        L.gpu_gaussian_noise(P(d), ctypes.c_float(0.5), ctypes.c_float(2.0), n)
+        x = d.cpu().numpy().astype(np.float64)
+        L.gpu_gaussian_noise(P(d), ctypes.c_float(0.5), ctypes.c_float(2.0), n)
+        y = d.cpu().numpy().astype(np.float64)
+        assert abs(x.mean() - 0.5) < 6 * 2.0 / np.sqrt(n)
+        assert abs(x.std() - 2.0) < 0.01
+        assert abs(np.corrcoef(x[:-1], x[1:])[0, 1]) < 0.01
+        assert abs(np.corrcoef(x, y)[0, 1]) < 0.01
+        z = (x - 0.5) / 2.0
+        assert abs((z ** 4).mean() - 3.0) < 0.05  # Gaussian kurtosis
+
+
+def test_memory_entry_points(libs, cuda):
+    n = 1001
+    a = rnd(n, 70)
+    for L in libs:
+        d = L.new_gpu_array(n)
+        assert d
+        assert L.gpu_array_get(d, 0) == 0.0  # zero-filled (gpu_mem.cu:28-36)
+        L.memcpy_to_gpu(a.ctypes.data, d, n)
+        e = L.new_gpu_array(n)
+        L.memcpy_on_gpu(d, e, n)
+        back = np.zeros(n, np.float32)
+        L.memcpy_gpu_dir(e, back.ctypes.data, n, 3)
+        assert np.array_equal(back, a)
+        L.gpu_zero(e, n)
+        L.memcpy_from_gpu(e, back.ctypes.data, n)
+        assert not back.any()
+        L.free_gpu_array(d)
+        L.free_gpu_array(e)

@@ -224,6 +224,8 @@ MMX = {
                                         ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_longlong)]),
     "mmx_solver_set_hext": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "mmx_solver_energy": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    "mmx_solver_relax": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong),
+                                        ctypes.POINTER(ctypes.c_float), ctypes.c_void_p]),
     "mmx_solver_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_float, ctypes.c_void_p, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_int), ctypes.c_longlong, ctypes.c_void_p]),
     "mmx_solver_m_device": (ctypes.c_void_p, [ctypes.c_void_p]),
@@ -443,6 +445,12 @@ class Solver:
         e = ctypes.c_double()
         _check(lib().mmx_solver_energy(self.h, ctypes.byref(e), stream))
         return e.value
+
+    def relax(self, max_steps=1000000, stream=None):
+        """Sim.Relax: returns (steps taken, last energy) (mmx_solver_relax)."""
+        k, e = ctypes.c_longlong(), ctypes.c_float()
+        _check(lib().mmx_solver_relax(self.h, max_steps, ctypes.byref(k), ctypes.byref(e), stream))
+        return k.value, e.value
 
     def run(self, seconds, period, max_rows=100000, max_steps=0, stream=None):
         """Sim.Run for 'seconds' with a table row every 'period' seconds:

@@ -603,7 +603,7 @@ void gpu_copy_unpad2D(float* source, float* dest, int S1, int S2, int D1, int D2
 }
 
 // ---------------------------------------------------------------------
-// FFT plan (gpu_fft0.cu:118-199) on the engine's zero-aware passes
+// FFT plan (gpu_fft0.cu:33-109) on the engine's zero-aware passes
 // ---------------------------------------------------------------------
 gpuFFT3dPlan* new_gpuFFT3dPlan_padded(int* size, int* paddedSize) {
   ABI_ASSERT(paddedSize[0] > 0 && paddedSize[1] > 1 && paddedSize[2] > 1, "new_gpuFFT3dPlan_padded");

@@ -1,7 +1,7 @@
 // Demagnetising kernel generation on the GPU.
 //
-// Restates FaceKernel6 / faceIntegral (src/go/sim/demag.go:127-185,
-// 243-284) and Exch6NgbrKernel (src/go/sim/exchange.go:328-353) with the
+// Restates FaceKernel6 / faceIntegral (src/go/sim/demag.go:26-84,
+// 142-183) and Exch6NgbrKernel (src/go/sim/exchange.go:44-71) with the
 // same float32 operations in the same order, so the real-space kernel is
 // bit-identical to the one the reference's Go subprocess computes
 // (mumaxkern-go, src/go/kernel-main/main.go:43): every product, sum,
@@ -115,7 +115,7 @@ __global__ void k_face_kernel6(float* __restrict__ k6, FaceKernelArgs a) {
 // Exch6NgbrKernel folded into the diagonal components (init.go:256-267).
 // The seven stencil cells are written in Go's order so that, when two
 // wrap onto the same cell (a dimension of size 1 or 2), the last write
-// wins, as in exchange.go:342-349; the tensor is then added.
+// wins, as in exchange.go:58-65; the tensor is then added.
 __global__ void k_add_exch6(float* __restrict__ k6, int P0, int P1, int P2, float c0, float c1, float c2) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const int64_t n3 = (int64_t)P0 * P1 * P2;

@@ -206,7 +206,7 @@ static void convolve(mmxd_sim* s, float* m, float* h) {
   for (int i = 0; i < 3; i++) L->inv(s->plan, s->buf[i], h + (int64_t)i * s->n);
 }
 
-// calcHeff (field.go:427-433): conv + local fields
+// calcHeff (field.go:74-80): conv + local fields
 static void calc_heff(mmxd_sim* s, float* m, float* h) {
   convolve(s, m, h);
   float K[3] = {s->anisK[0], s->anisK[1], s->anisK[2]};
@@ -224,7 +224,7 @@ extern "C" mmxd_sim* mmxd_new(mmxd_lib* L, const mmxd_config* cfg, const float* 
   mmxd_sim* s = new mmxd_sim();
   s->L = L;
   s->cfg = *cfg;
-  // initMaterial / units (init.go:80-113, material.go:338-366)
+  // initMaterial / units (init.go:80-113, material.go:51-111)
   float mu0 = (float)(4.0e-7 * M_PI), gamma0 = 2.211e5f;
   float ms = (float)cfg->msat, A = (float)cfg->aexch;
   float t = f_mul(f_mul(mu0, ms), ms);
@@ -239,7 +239,7 @@ extern "C" mmxd_sim* mmxd_new(mmxd_lib* L, const mmxd_config* cfg, const float* 
     s->per[d] = cfg->periodic[2 - d];
     s->cs[d] = f_div((float)cfg->cell[2 - d], s->unitL);
     s->P[d] = (s->N[d] > 1 && s->per[d] == 0) ? 2 * s->N[d] : s->N[d];  // padSize (kernel.go:80-90)
-    s->hext[d] = f_div((float)cfg->bext[2 - d], s->unitB);              // updateHext (field.go:403-414)
+    s->hext[d] = f_div((float)cfg->bext[2 - d], s->unitB);              // updateHext (field.go:50-61)
   }
   s->alpha = (float)cfg->alpha;
   s->anis = cfg->anis_type;

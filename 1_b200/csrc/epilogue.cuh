@@ -27,6 +27,8 @@ struct EpiArgs {
   const float* aux0;
   const float* aux1;
   float* err;           // device scalar (maxabs target), may be null
+  double* energy;       // RK stages: device accumulator of the total energy
+                        // density sum (Relax's energy, relax.go:14-23), may be null
   const float* dt_dev;  // RK: device dt
   float* kbuf[RK_MAXS]; // RK: stage torques
   int stage;            // RK: index of this stage's k
@@ -65,24 +67,36 @@ __device__ __forceinline__ void epi_load(const EpiArgs& ea, int64_t g, EpiIn<MOD
 
 // next: if not null, receives the cell's next stage input (Heun: m1est
 // after the predictor, m after the corrector)
+// eacc: the thread's energy-density sum (RK stages with ea.energy set)
 template <int MODE>
 __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float hx, float hy, float hz,
-                                            const EpiIn<MODE>& in, float& lmax, float* next = nullptr);
+                                            const EpiIn<MODE>& in, float& lmax, float* next = nullptr,
+                                            double* eacc = nullptr);
 
 // cell g (index into one component), field (hx,hy,hz) from the convolution
 template <int MODE>
-__device__ __forceinline__ void epi_cell(const EpiArgs& ea, int64_t g, float hx, float hy, float hz, float& lmax) {
+__device__ __forceinline__ void epi_cell(const EpiArgs& ea, int64_t g, float hx, float hy, float hz, float& lmax,
+                                         double* eacc = nullptr) {
   EpiIn<MODE> in;
   epi_load<MODE>(ea, g, in);
-  epi_cell_in<MODE>(ea, g, hx, hy, hz, in, lmax);
+  epi_cell_in<MODE>(ea, g, hx, hy, hz, in, lmax, nullptr, eacc);
 }
 
 template <int MODE>
 __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float hx, float hy, float hz,
-                                            const EpiIn<MODE>& in, float& lmax, float* next) {
+                                            const EpiIn<MODE>& in, float& lmax, float* next, double* eacc) {
     const int64_t n = ea.n;
     float mx = in.m[0], my = in.m[1], mz = in.m[2];
     llg_local(ea.lf, mx, my, mz, hx, hy, hz);
+    if constexpr (MODE == EPI_RK || MODE == EPI_TORQUE) {
+      // energy density of the stage's m: -1/2 m.h_conv - m.Hext - 1/2 K (m.u)^2
+      // = -1/2 m.(h + Hext) with h the full field (the anisotropy terms
+      // cancel), summed in float64
+      if (ea.energy && eacc) {
+        float s = FA(FA(FM(mx, FA(hx, ea.lf.hext[0])), FM(my, FA(hy, ea.lf.hext[1]))), FM(mz, FA(hz, ea.lf.hext[2])));
+        *eacc += (double)FM(-0.5f, s);
+      }
+    }
     if (MODE == EPI_FIELD) {
       ea.out0[g] = hx;
       ea.out0[n + g] = hy;
@@ -96,7 +110,7 @@ __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float 
       ea.out0[2 * n + g] = hz;
       if (ea.err) lmax = fmaxf(lmax, fmaxf(fabsf(hx), fmaxf(fabsf(hy), fabsf(hz))));
     } else if (MODE == EPI_HEUN1) {
-      // t0 = torque*dt; m1est = normalize(m + t0)   (adaptive_heun.go:141-146)
+      // t0 = torque*dt; m1est = normalize(m + t0)   (adaptive_heun.go:39-44)
       ea.out0[g] = hx;
       ea.out0[n + g] = hy;
       ea.out0[2 * n + g] = hz;
@@ -107,7 +121,7 @@ __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float 
       ea.out1[2 * n + g] = ez;
       if (next) { next[0] = ex; next[1] = ey; next[2] = ez; }
     } else if (MODE == EPI_HEUN2) {
-      // t = 0.5 t1 + 0.5 t0; m = normalize(m + t)   (adaptive_heun.go:148-154)
+      // t = 0.5 t1 + 0.5 t0; m = normalize(m + t)   (adaptive_heun.go:46-52)
       float tx = FA(FM(0.5f, hx), FM(0.5f, in.a0[0]));
       float ty = FA(FM(0.5f, hy), FM(0.5f, in.a0[1]));
       float tz = FA(FM(0.5f, hz), FM(0.5f, in.a0[2]));
@@ -118,7 +132,7 @@ __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float 
       ea.out0[2 * n + g] = nz;
       if (next) { next[0] = nx; next[1] = ny; next[2] = nz; }
       if (ea.err) {
-        // error = maxabs(m1est - m)   (adaptive_heun.go:158-160)
+        // error = maxabs(m1est - m)   (adaptive_heun.go:56-59)
         float d0 = fabsf(FA(mx, FM(-1.f, nx)));
         float d1 = fabsf(FA(my, FM(-1.f, ny)));
         float d2 = fabsf(FA(mz, FM(-1.f, nz)));
@@ -174,11 +188,18 @@ __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float 
   
 }
 
-// block-wide maximum of lmax into *ea.err (non-negative float atomics)
+// block-wide maximum of lmax into *ea.err (non-negative float atomics) and,
+// for RK stages, the warp sums of the energy density into *ea.energy
 template <int MODE>
-__device__ __forceinline__ void epi_flush_max(const EpiArgs& ea, float lmax) {
+__device__ __forceinline__ void epi_flush_max(const EpiArgs& ea, float lmax, double eacc = 0.0) {
   if ((MODE == EPI_HEUN2 || MODE == EPI_RK || MODE == EPI_TORQUE) && ea.err) {
     for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
     if ((threadIdx.x & 31) == 0) atomic_max_nonneg(ea.err, lmax);
+  }
+  if constexpr (MODE == EPI_RK || MODE == EPI_TORQUE) {
+    if (ea.energy) {
+      for (int o = 16; o > 0; o >>= 1) eacc += __shfl_xor_sync(0xffffffffu, eacc, o);
+      if ((threadIdx.x & 31) == 0) atomicAdd(ea.energy, eacc);
+    }
   }
 }

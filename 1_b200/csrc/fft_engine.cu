@@ -5,7 +5,7 @@
 //   real data  (N0, N1, N2)                  -- one magnetisation component
 //   spectrum   (P0, P1, HZ) complex,  HZ = P2/2 + 1
 // which is exactly the in-place cuFFT R2C layout the reference uses:
-// buffer of (P0, P1, P2+2) floats (gpu_fft0.cu:147-153,181-194).
+// buffer of (P0, P1, P2+2) floats (gpu_fft0.cu:57-59,96-109).
 //
 // Passes (one kernel each):
 //   Z  : real rows -> half spectrum, via a complex FFT of length P2/2 on

@@ -515,6 +515,7 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
     MidRows<M, 1, NST, NL, T, PITCH, true, QK>::run(sm, tw);
   }
   float lmax = 0.f;
+  double eacc = 0.0;
   const int64_t g0 = (int64_t)r0 * N2;
   if (N2 == M) {
     // open boundary along Z: the row has exactly M cells.  Every per-cell
@@ -545,7 +546,7 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
         w[2 * PITCH] = nm[1];
         w[4 * PITCH] = nm[2];
       } else {
-        epi_cell_in<MODE>(ea, g0 + e, hx, hy, hz, in[i], lmax);
+        epi_cell_in<MODE>(ea, g0 + e, hx, hy, hz, in[i], lmax, nullptr, &eacc);
       }
     }
     if constexpr (FUSE) {
@@ -601,10 +602,10 @@ __device__ __forceinline__ void zinv_body(const ZinvArgs& za, int bx) {
       float hx = (zz & 1) ? base[0].y : base[0].x;
       float hy = (zz & 1) ? base[PITCH].y : base[PITCH].x;
       float hz = (zz & 1) ? base[2 * PITCH].y : base[2 * PITCH].x;
-      epi_cell<MODE>(ea, g0 + e, hx, hy, hz, lmax);
+      epi_cell<MODE>(ea, g0 + e, hx, hy, hz, lmax, &eacc);
     }
   }
-  epi_flush_max<MODE>(ea, lmax);
+  epi_flush_max<MODE>(ea, lmax, eacc);
 }
 
 template <int M, int RT, int T, int MODE>

@@ -11,7 +11,7 @@
 // The scratch array is a file-scope __device__ array: every GPU that loads
 // the library holds its 8 KB until the process exits.  In host code the
 // name g_reduce_scratch is only a host-side stand-in, not a device address;
-// the device address is obtained once per device with
+// the device address is obtained once per device (per CUDA context) with
 // cudaGetSymbolAddress (the first call on a device does it, with that
 // device current) and passed to the kernels.
 //
@@ -83,9 +83,22 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_final(int op, const double* _
   if (threadIdx.x == 0) out[0] = (float)v;
 }
 
-// device address of g_reduce_scratch, per device, set up on first use
+// Device address of g_reduce_scratch, looked up once per CUDA context (the
+// module, and so the array, is loaded per context: a context created anew,
+// e.g. after cudaDeviceReset, holds it at a new address).  The context is
+// read with the driver's cuCtxGetCurrent, reached through the runtime's
+// entry-point table so the library does not link the driver library; the
+// call is legal while another thread captures a graph.
+typedef int (*ctx_get_fn)(void**);
 static std::mutex g_rs_mu;
-static double* g_rs_addr[64] = {nullptr};
+struct RsEntry {
+  void* ctx;
+  int dev;
+  double* addr;
+};
+static RsEntry g_rs_cache[64];
+static int g_rs_n = 0;
+static ctx_get_fn g_ctx_get = nullptr;
 
 static int rs_scratch(double** out) {
   int dev = 0;
@@ -94,21 +107,49 @@ static int rs_scratch(double** out) {
     mmx_set_error(cudaGetErrorString(e));
     return MMX_ERR_CUDA;
   }
-  if (dev < 0 || dev >= 64) {
-    mmx_set_error("mmx_reduce_static: device index out of range");
-    return MMX_ERR_ARG;
-  }
   std::lock_guard<std::mutex> lk(g_rs_mu);
-  if (!g_rs_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_reduce_scratch);
-    if (e != cudaSuccess || p == nullptr) {
-      mmx_set_error(e != cudaSuccess ? cudaGetErrorString(e) : "mmx_reduce_static: no symbol address");
+  if (!g_ctx_get) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !f) {
+      mmx_set_error("mmx_reduce_static: cuCtxGetCurrent not available");
       return MMX_ERR_CUDA;
     }
-    g_rs_addr[dev] = (double*)p;
+    g_ctx_get = (ctx_get_fn)f;
   }
-  *out = g_rs_addr[dev];
+  // A thread that has made no runtime call yet has no context bound (the
+  // runtime binds the device's primary context at its first launch): it
+  // uses the device's entry, which is the primary context's.
+  void* ctx = nullptr;
+  if (g_ctx_get(&ctx) != 0) ctx = nullptr;
+  for (int i = 0; i < g_rs_n; i++)
+    if (g_rs_cache[i].dev == dev && (!ctx || g_rs_cache[i].ctx == ctx)) {
+      *out = g_rs_cache[i].addr;
+      return MMX_OK;
+    }
+  // set-up: looks the array up (loading the module into the context if
+  // needed), then records the context it belongs to
+  void* p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_reduce_scratch);
+  if (e != cudaSuccess || p == nullptr) {
+    mmx_set_error(e != cudaSuccess ? cudaGetErrorString(e) : "mmx_reduce_static: no symbol address");
+    return MMX_ERR_CUDA;
+  }
+  if (g_ctx_get(&ctx) != 0) ctx = nullptr;
+  // replace a stale entry of this device (an earlier context), else append
+  int slot = -1;
+  for (int i = 0; i < g_rs_n; i++)
+    if (g_rs_cache[i].dev == dev) slot = i;
+  if (slot < 0) {
+    if (g_rs_n == 64) {
+      mmx_set_error("mmx_reduce_static: too many devices");
+      return MMX_ERR_ARG;
+    }
+    slot = g_rs_n++;
+  }
+  g_rs_cache[slot] = RsEntry{ctx, dev, (double*)p};
+  *out = (double*)p;
   return MMX_OK;
 }
 

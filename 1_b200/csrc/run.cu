@@ -143,10 +143,6 @@ void solver_run_free(mmx_solver* s) {
   s->rows_cap = 0;
 }
 
-// cell volume as the reference's float32 product (energy.go:38-44)
-static float cell_volume(const mmx_solver* s) {
-  return f32_mul(f32_mul(s->p.cellsize[0], s->p.cellsize[1]), s->p.cellsize[2]);
-}
 
 extern "C" int mmx_solver_energy(mmx_solver* s, double* energy, cudaStream_t st) {
   if (!s || !energy) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
@@ -163,7 +159,7 @@ extern "C" int mmx_solver_energy(mmx_solver* s, double* energy, cudaStream_t st)
   double sum = 0;
   MMX_TRY(cudaMemcpyAsync(&sum, s->eacc, sizeof(double), cudaMemcpyDeviceToHost, st));
   MMX_TRY(cudaStreamSynchronize(st));
-  *energy = sum * (double)cell_volume(s);
+  *energy = sum * (double)solver_cell_volume(s);
   return MMX_OK;
 }
 
@@ -316,5 +312,42 @@ extern "C" int mmx_solver_run(mmx_solver* s, double seconds, float period, float
     mmx_set_error("run: trial cap reached before the stop time");
     return MMX_ERR_STATE;
   }
+  return MMX_OK;
+}
+
+// Sim.Relax (relax.go:14-23): the energy is wanted from now on (and stays
+// wanted, as in the reference), one step, then steps while the energy the
+// RK steps compute does not rise; the steps themselves reject a trial whose
+// energy rose (rk.go:297-301,425).  The energies are compared in float32.
+extern "C" int mmx_solver_relax(mmx_solver* s, long long max_steps, long long* steps, float* energy,
+                                cudaStream_t st) {
+  if (!s || max_steps < 1) { mmx_set_error("bad argument"); return MMX_ERR_ARG; }
+  if (s->p.solver == MMX_SOLVER_HEUN) {
+    mmx_set_error("relax: the heun step computes no energy; use an RK solver");
+    return MMX_ERR_ARG;
+  }
+  if (s->devctl) {
+    mmx_set_error("relax: turn the device dt controller off first");
+    return MMX_ERR_STATE;
+  }
+  if (!s->eacc && cudaMalloc(&s->eacc, sizeof(double)) != cudaSuccess) {
+    mmx_set_error("out of device memory");
+    return MMX_ERR_MEM;
+  }
+  s->want_energy = 1;
+  long long k = 0;
+  MMX_CHECK_RC(solver_step_once(s, st));
+  s->steps++;
+  k++;
+  float prevE = f32_add(s->energy, 1.f);
+  while (s->energy <= prevE && k < max_steps) {
+    prevE = s->energy;
+    MMX_CHECK_RC(solver_step_once(s, st));
+    s->steps++;
+    k++;
+  }
+  MMX_TRY(cudaStreamSynchronize(st));
+  if (steps) *steps = k;
+  if (energy) *energy = s->energy;
   return MMX_OK;
 }

@@ -207,6 +207,7 @@ __global__ void FFT_BOUNDS(THREADS) k_zinv_epi(const float2* __restrict__ S, Lin
   tile_fft<EPT, POW2>(sm, fz, nl, 1, ld, false, true);
 
   float lmax = 0.f;
+  double eacc = 0.0;
   for (int e = threadIdx.x; e < nr * N2; e += nt) {
     int r = e / N2, z = e - r * N2;
     int64_t g = (int64_t)(r0 + r) * N2 + z;
@@ -214,9 +215,9 @@ __global__ void FFT_BOUNDS(THREADS) k_zinv_epi(const float2* __restrict__ S, Lin
     float hx = (z & 1) ? base[0].y : base[0].x;
     float hy = (z & 1) ? base[ld].y : base[ld].x;
     float hz = (z & 1) ? base[2 * ld].y : base[2 * ld].x;
-    epi_cell<MODE>(ea, g, hx, hy, hz, lmax);
+    epi_cell<MODE>(ea, g, hx, hy, hz, lmax, &eacc);
   }
-  epi_flush_max<MODE>(ea, lmax);
+  epi_flush_max<MODE>(ea, lmax, eacc);
 }
 
 // ---------------------------------------------------------------------
@@ -324,7 +325,22 @@ struct ScopedPass {
   cudaStream_t st;
   PassTimer* t = nullptr;
   cudaEvent_t a = nullptr, b = nullptr;
+  const char* nm = nullptr;
   ScopedPass(mmx_solver* s_, const char* name, cudaStream_t st_) : s(s_), st(st_) {
+    if (s->capture_events) {
+      // inside the capture of the profiling graph: event-record nodes,
+      // chained (a pass starts at the previous pass's end event) so a step
+      // of n passes carries n + 1 event nodes
+      nm = name;
+      cudaEventCreate(&b);
+      if (s->gevents.empty()) {
+        cudaEventCreate(&a);
+        cudaEventRecordWithFlags(a, st, cudaEventRecordExternal);
+      } else {
+        a = s->gevents.back().b;
+      }
+      return;
+    }
     if (!s->profile) return;
     t = timer_for(s, name);
     cudaEventCreate(&a);
@@ -332,6 +348,11 @@ struct ScopedPass {
     cudaEventRecord(a, st);
   }
   ~ScopedPass() {
+    if (nm) {
+      cudaEventRecordWithFlags(b, st, cudaEventRecordExternal);
+      s->gevents.push_back({nm, a, b, s->gevents.empty()});
+      return;
+    }
     if (!t) return;
     cudaEventRecord(b, st);
     t->pending.push_back({a, b});
@@ -644,6 +665,8 @@ static cudaError_t rk_stage(mmx_solver* s, int i, cudaStream_t st, float* dt_dev
   ea.dt_dev = dt_dev;
   for (int j = 0; j < s->stages; j++) ea.kbuf[j] = s->kb[j];
   ea.stage = i;
+  // calcHeffEnergy at the last stage (FSAL) or the first (rk.go:321-337)
+  if (s->want_energy && s->eacc && (s->fsal ? i == s->stages - 1 : i == 0)) ea.energy = s->eacc;
   if (i == s->stages - 1) {
     // last stage: k_last, then m_high (b) and, if adaptive, m_low (b2)
     ea.out0 = s->kb[i];
@@ -727,9 +750,16 @@ static int rk_step(mmx_solver* s, cudaStream_t st) {
   const bool bounds = s->p.min_dm != 0.f || s->p.max_dm != 0.f || s->p.min_dt != 0.f || s->p.max_dt != 0.f;
   double time0 = s->time;
   int good = 0, trials = 0;
+  const bool want_e = s->want_energy && s->eacc;
+  const int e_stage = s->fsal ? s->stages - 1 : 0;
+  // energy must not rise when it is wanted (rk.go:297-301,425)
+  float prevE = s->energy;
+  if (prevE == 0.f) prevE = 9999999999.f;
   while (!good && trials < 10) {
     trials++;
     for (int i = 0; i < s->stages; i++) {
+      if (want_e && i == e_stage && !(s->fsal && i == 0 && s->fsal_init))
+        MMX_TRY(cudaMemsetAsync(s->eacc, 0, sizeof(double), st));
       if (s->fsal && i == 0 && s->fsal_init) {
         // FSAL copy k0 <- k_last (rk.go:311-315), done as a buffer swap.
         // The reference repeats it on a retry, so the retry starts from the
@@ -765,15 +795,22 @@ static int rk_step(mmx_solver* s, cudaStream_t st) {
       }
     }
     s->time = time0 + (double)s->dt;
+    double esum = 0;
+    if (want_e) MMX_TRY(cudaMemcpyAsync(&esum, s->eacc, sizeof(double), cudaMemcpyDeviceToHost, st));
     if (!s->adaptive) {
       good = 1;
       int one = 1;
       MMX_TRY(cudaMemcpyAsync(acc_dev, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+      if (want_e) {
+        MMX_TRY(cudaStreamSynchronize(st));
+        s->energy = (float)(esum * (double)solver_cell_volume(s));
+      }
       break;
     }
     float sc[2];
     MMX_TRY(cudaMemcpyAsync(sc, s->scratch, sizeof(float) * 2, cudaMemcpyDeviceToHost, st));
     MMX_TRY(cudaStreamSynchronize(st));
+    if (want_e) s->energy = (float)(esum * (double)solver_cell_volume(s));
     float err = sc[0];
     s->torque = sc[1];
     s->step_error = err;
@@ -782,7 +819,7 @@ static int rk_step(mmx_solver* s, cudaStream_t st) {
     if (factor < 0.01f) factor = 0.01f;
     s->dt = f32_mul(s->dt, factor);
     if (s->dt != s->dt || err != err) { mmx_set_error("dt = NaN"); return MMX_ERR_NAN; }
-    if (err > f32_mul(2.f, s->p.max_error)) {
+    if (err > f32_mul(2.f, s->p.max_error) || (want_e && s->energy > prevE)) {
       good = 0;
     } else {
       good = 1;
@@ -844,9 +881,11 @@ extern "C" int mmx_face_kernel6(const int P[3], const int periodic[3], const flo
   return MMX_OK;
 }
 
+static void free_profile_graph(mmx_solver* s);
 static void solver_free(mmx_solver* s) {
   if (!s) return;
   solver_run_free(s);
+  free_profile_graph(s);
   if (s->gexec) cudaGraphExecDestroy(s->gexec);
   for (int g = 0; g < 2; g++)
     if (s->dgraph[g]) cudaGraphExecDestroy(s->dgraph[g]);
@@ -882,7 +921,7 @@ extern "C" int mmx_solver_create(const mmx_params* p, mmx_solver** out) {
   }
   if (s->N[2] < 2 || s->N[1] < 2) {
     delete s;
-    mmx_set_error("internal Y and Z sizes must be >= 2 (gpu_fft0.cu:124-126)");
+    mmx_set_error("internal Y and Z sizes must be >= 2 (gpu_fft0.cu:39-41)");
     return MMX_ERR_SIZE;
   }
   s->is2d = s->P[0] == 1;
@@ -1022,6 +1061,12 @@ int solver_field_conv(mmx_solver* s, const float* m, float* h, cudaStream_t st) 
   }
   if (e != cudaSuccess) { mmx_set_error(cudaGetErrorString(e)); return MMX_ERR_CUDA; }
   return MMX_OK;
+}
+
+static int step_once(mmx_solver* s, cudaStream_t st);
+int solver_step_once(mmx_solver* s, cudaStream_t st) { return step_once(s, st); }
+float solver_cell_volume(const mmx_solver* s) {
+  return f32_mul(f32_mul(s->p.cellsize[0], s->p.cellsize[1]), s->p.cellsize[2]);
 }
 
 static int step_once(mmx_solver* s, cudaStream_t st) {
@@ -1248,11 +1293,74 @@ static cudaError_t step_launches(mmx_solver* s, cudaStream_t st) {
   return s->p.solver == MMX_SOLVER_HEUN ? heun_step(s, st) : rk_fixed_launches(s, st);
 }
 
+static void free_profile_graph(mmx_solver* s) {
+  if (s->pgexec) cudaGraphExecDestroy(s->pgexec);
+  s->pgexec = nullptr;
+  for (auto& g : s->gevents) {
+    if (g.own_a) cudaEventDestroy(g.a);
+    cudaEventDestroy(g.b);
+  }
+  s->gevents.clear();
+}
+
+// Fixed-step solvers with profile mode 2: each step replays a graph whose
+// passes are bracketed by event-record nodes; after each replay the pass
+// times are added to the timers.
+static int profiled_graph_steps(mmx_solver* s, int nsteps, cudaStream_t st) {
+  for (int k = 0; k < nsteps; k++) {
+    if (heun_fused(s) && !s->spec_ready) {
+      cudaError_t e = zfwd_only(s, s->m, st);
+      if (e != cudaSuccess) { mmx_set_error(cudaGetErrorString(e)); return MMX_ERR_CUDA; }
+      s->spec_ready = 1;
+    }
+    if (!s->pgexec || s->pgstream != st) {
+      free_profile_graph(s);
+      cudaStream_t cap = st;
+      bool own = false;
+      if (cap == 0) { MMX_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)); own = true; }
+      cudaGraph_t g;
+      MMX_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+      s->capture_events = 1;
+      cudaError_t e = step_launches(s, cap);
+      s->capture_events = 0;
+      cudaError_t e2 = cudaStreamEndCapture(cap, &g);
+      if (own) cudaStreamDestroy(cap);
+      if (e != cudaSuccess || e2 != cudaSuccess) { mmx_set_error("graph capture failed"); return MMX_ERR_CUDA; }
+      MMX_TRY(cudaGraphInstantiate(&s->pgexec, g, 0));
+      cudaGraphDestroy(g);
+      s->pgstream = st;
+    }
+    MMX_TRY(cudaGraphLaunch(s->pgexec, st));
+    MMX_TRY(cudaStreamSynchronize(st));
+    for (auto& g : s->gevents) {
+      float ms = 0;
+      MMX_TRY(cudaEventElapsedTime(&ms, g.a, g.b));
+      PassTimer* t = timer_for(s, g.name.c_str());
+      t->ms += ms;
+      t->launches++;
+    }
+    s->time += (double)s->dt;
+    s->steps++;
+  }
+  return MMX_OK;
+}
+
 extern "C" int mmx_solver_step(mmx_solver* s, int nsteps, cudaStream_t st) {
   if (!s || nsteps < 0) { mmx_set_error("bad argument"); return MMX_ERR_ARG; }
   if (s->devctl) return rk_device_steps(s, nsteps, st);
-  bool graphable = s->use_graph && !s->profile &&
-                   ((s->p.solver == MMX_SOLVER_HEUN && s->p.max_error == 0.f) || rk_fixed(s));
+  const bool fixed_graphable = (s->p.solver == MMX_SOLVER_HEUN && s->p.max_error == 0.f) || rk_fixed(s);
+  if (s->profile == 2 && fixed_graphable && !s->want_energy) {
+    if (s->p.solver != MMX_SOLVER_HEUN && s->dt_uploaded != s->dt) {
+      float v[2] = {s->dt, 0.f};
+      int one = 1;
+      memcpy(&v[1], &one, sizeof(int));
+      MMX_TRY(cudaMemcpyAsync(s->scratch + 2, v, sizeof(v), cudaMemcpyHostToDevice, st));
+      MMX_TRY(cudaStreamSynchronize(st));
+      s->dt_uploaded = s->dt;
+    }
+    return profiled_graph_steps(s, nsteps, st);
+  }
+  bool graphable = s->use_graph && !s->profile && !s->want_energy && fixed_graphable;
   if (graphable && s->p.solver != MMX_SOLVER_HEUN && s->dt_uploaded != s->dt) {
     float v[2] = {s->dt, 0.f};
     int one = 1;

@@ -72,9 +72,22 @@ struct mmx_solver {
   cudaGraphExec_t rungraph = nullptr;     // devctl: WHILE-conditional run graph
   cudaStream_t rungraph_stream = nullptr;
   double* eacc = nullptr;                 // energy accumulator (one double)
-  // profiling
+  int want_energy = 0;                    // Sim.wantEnergy: RK steps compute the energy (Relax)
+  float energy = 0.f;                     // Sim.energy: the last energy an RK step computed
+  // profiling: 1 = events around each launch of directly launched steps;
+  // 2 = event-record nodes inside the captured step graph (per-pass times
+  // as the graph runs them)
   int profile = 0;
   std::vector<PassTimer> timers;
+  int capture_events = 0;  // ScopedPass records graph event nodes
+  struct GraphEvent {
+    std::string name;
+    cudaEvent_t a, b;  // a is the previous pass's b when chained
+    bool own_a;
+  };
+  std::vector<GraphEvent> gevents;
+  cudaGraphExec_t pgexec = nullptr;  // the step graph with event nodes
+  cudaStream_t pgstream = nullptr;
 };
 
 // Host float32 arithmetic (one rounding per operation; x86-64 SSE, no
@@ -96,3 +109,7 @@ cudaError_t solver_device_trial(mmx_solver* s, cudaStream_t st, bool first);
 int solver_device_download(mmx_solver* s);
 // Frees the run loop's buffers and graph (run.cu).
 void solver_run_free(mmx_solver* s);
+// One solver step (host controller), as mmx_solver_step takes it.
+int solver_step_once(mmx_solver* s, cudaStream_t st);
+// Cell volume as the reference's float32 product (energy.go:38-44).
+float solver_cell_volume(const mmx_solver* s);

@@ -470,13 +470,50 @@ def run_adaptive(args, name):
     print(json.dumps(line), flush=True)
 
 
+def kernel_host(eng, torch, params):
+    """The real-space demag + exchange kernel of the padded grid, built on
+    the GPU (mmx_face_kernel6), as the host array the driver restatement
+    takes."""
+    N = tuple(params.size)
+    per = tuple(params.periodic)
+    Pd = tuple(2 * n if (n > 1 and p == 0) else n for n, p in zip(N, per))
+    out = torch.zeros((6,) + Pd, device="cuda")
+    eng.face_kernel6_device(Pd, per, [params.cellsize[d] for d in range(3)], exch6=True,
+                            out_ptr=ctypes.c_void_p(out.data_ptr()))
+    torch.cuda.synchronize()
+    k = out.cpu().numpy()
+    del out
+    return k
+
+
+def time_driver(eng, torch, w, m0, libpath, steps=20, warmup=2):
+    """Whole-grid steps per second of a libgpukern implementation driven by
+    the Go-driver restatement (libmmxdriver.so): every primitive call is
+    synchronous, as in the reference, so the wall clock around the steps is
+    the device time plus the launch gaps the call sequence imposes."""
+    kw = sim_kwargs(w)
+    k6 = kernel_host(eng, torch, eng.mmx_params(**kw))
+    d = eng.DriverSim(eng.driver_config(**kw), m0, k6, libpath=libpath)
+    d.steps(warmup)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    d.steps(steps)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    d.close()
+    n = int(np.prod(w["grid"]))
+    return {"value": n * steps / el, "unit": "cell-steps/s", "ms_per_step": 1e3 * el / steps, "steps": steps,
+            "warmup": warmup, "library": os.path.relpath(libpath, ROOT),
+            "path": "Go-driver restatement (libmmxdriver.so) over the libgpukern C ABI, synchronous calls"}
+
+
 def run_reference(args, w, name):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     cb = cpu_baseline(w)
     # a bounded sample: the whole-grid steps actually timed, not --steps
-    line = {"metric": "cell-steps/s", "value": cb["value"], "unit": "cell-steps/s", "n_gpus": args.gpus,
+    line = {"metric": "cell-steps/s", "value": cb["value"], "unit": "cell-steps/s", "n_gpus": 1,
             "steps": cb["steps_timed"], "warmup": 1, "steps_requested": args.steps,
             "warmup_requested": args.warmup, "ms_per_step": 1e3 * np.prod(w["grid"]) / cb["value"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -485,6 +522,25 @@ def run_reference(args, w, name):
                        "parallelism": "host threads (rank 0)"},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    # context: the reference's own CUDA library (cuFFT, synchronous
+    # primitives), built from its sources for sm_100a, driven by the
+    # Go-driver restatement on the same workload
+    ref_lib = os.path.join(ROOT, "oracle", "_ref", "libgpukern_ref.so")
+    if args.no_reference_gpu:
+        pass
+    elif not os.path.exists(ref_lib):
+        line["reference_gpu"] = {"unavailable": "oracle/_ref/libgpukern_ref.so was not built"}
+    else:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                eng = importlib.import_module("1_b200")
+                m0 = seeded_m(w["grid"], w["seed"], w["init"])
+                line["reference_gpu"] = time_driver(eng, torch, w, m0, ref_lib, steps=args.drop_in_steps)
+            else:
+                line["reference_gpu"] = {"unavailable": "no CUDA device"}
+        except Exception as e:  # context only: never fail the CPU arm
+            line["reference_gpu"] = {"unavailable": "%s: %s" % (type(e).__name__, e)}
     print(json.dumps(line), flush=True)
 
 
@@ -534,15 +590,20 @@ def run_ours(args, w, name):
     ms = float(t.item())
     value = world * n * args.steps / (ms / 1e3)
 
-    # ---- per-kernel durations with CUDA events on the step's stream ----
-    s.use_graph(False)
-    s.profile(True)
+    # ---- per-kernel durations: event-record nodes inside the step graph ----
+    s.profile(2)
     ksteps = min(args.steps, 200)
     s.step(ksteps, sh)
     torch.cuda.synchronize()
     times = s.pass_times()
     s.profile(False)
     barrier()
+
+    # ---- the drop-in path: this library's primitives under the Go-driver
+    # restatement (the call sequence the unchanged Go front end issues) ----
+    drop_in = None
+    if world == 1 and not args.no_drop_in:
+        drop_in = time_driver(eng, torch, w, m0, eng.LIB_PATH, steps=args.drop_in_steps)
 
     # ---- end to end through the C ABI with host buffers ----
     s.use_graph(True)
@@ -578,10 +639,17 @@ def run_ours(args, w, name):
     b, bytes_per_cell_step, state = pass_bytes(w)
     peak, peak_kind = measured_peaks()
     dom = max(times, key=lambda k: times[k][0])
-    dom_ms = times[dom][0] / times[dom][1]
+    # each event node between two passes adds a gap of its own (the next
+    # kernel cannot start before the event is recorded): the event-timed
+    # step exceeds the step timed without event nodes (the timed region
+    # above) by that gap per pass, which is taken off every pass equally
+    ev_step_ms = sum(v[0] for v in times.values()) / ksteps
+    passes_per_step = launches_per_step = sum(la for _, la in times.values()) / ksteps
+    gap_ms = max(0.0, (ev_step_ms - ms / args.steps) / passes_per_step) if passes_per_step else 0.0
+    per_launch = {k: v[0] / v[1] - gap_ms for k, v in times.items()}
+    dom_ms = per_launch[dom]
     achieved = b[dom] / (dom_ms / 1e3) / 1e9
     traffic = ncu_traffic(dom, name)
-    launches_per_step = sum(la for _, la in times.values()) / ksteps
     line = {
         "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -594,7 +662,12 @@ def run_ours(args, w, name):
                      "algorithmic_bytes_per_launch": b[dom], "avg_launch_ms": dom_ms,
                      "step_bytes_per_cell": bytes_per_cell_step,
                      "step_frac": bytes_per_cell_step * value / world / 1e9 / peak,
-                     "passes_ms_per_launch": {k: v[0] / v[1] for k, v in times.items()}},
+                     "passes_ms_per_launch": per_launch,
+                     "passes_timing": "event-record nodes between the passes inside the step graph (%d steps): "
+                                      "the event-timed step (%.4f ms) exceeds the %.4f ms step timed without "
+                                      "event nodes by %.4f ms per pass, taken off each pass" %
+                                      (ksteps, ev_step_ms, ms / args.steps, gap_ms),
+                     "passes_ms_per_launch_events": {k: v[0] / v[1] for k, v in times.items()}},
         "e2e": {"value": e2e, "unit": "cell-steps/s",
                 "h2d_bytes_per_step": 3 * n * 4 / args.steps,
                 "d2h_bytes_per_step": 12 + 3 * n * 4 / args.steps,
@@ -603,6 +676,8 @@ def run_ours(args, w, name):
         "gpu_launches": int(round(launches_per_step * args.steps)),
         "clocks": clk,
     }
+    if drop_in is not None:
+        line["drop_in"] = drop_in
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w)
     print(json.dumps(line), flush=True)
@@ -621,7 +696,16 @@ def main():
     ap.add_argument("--requests", type=int, default=16, help="serving: requests of the stream to run")
     ap.add_argument("--serve-max-steps", type=int, default=0, help="serving: step cap per relaxation (0: none)")
     ap.add_argument("--no-plain", action="store_true", help="serving: skip the one-at-a-time arm")
+    ap.add_argument("--no-drop-in", action="store_true", help="skip timing the drop-in primitive path")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="reference arm: skip timing the reference's own CUDA library")
+    ap.add_argument("--drop-in-steps", type=int, default=20)
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: start the ranks here when not under torchrun
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(args.gpus),
+               "--master-addr", "127.0.0.1", "--master-port", str(29500 + os.getpid() % 1000)] + sys.argv
+        sys.exit(subprocess.call(cmd))
     if args.workload in SERVE_WORKLOADS:
         if int(os.environ.get("WORLD_SIZE", "1")) > 1:
             import torch.distributed as dist

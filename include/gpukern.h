@@ -112,11 +112,11 @@ typedef struct gpuFFT3dPlan {
   void* engine;       /* B200 transform plan (opaque) */
 } gpuFFT3dPlan;       /* gpu_fft0.h:30-42 */
 gpuFFT3dPlan* new_gpuFFT3dPlan_padded(int* size, int* paddedSize); /* gpu_fft0.h:51 */
-gpuFFT3dPlan* new_gpuFFT3dPlan(int* size);                        /* gpu_fft0.cu:177 */
+gpuFFT3dPlan* new_gpuFFT3dPlan(int* size);                        /* gpu_fft0.cu:92-94 */
 void delete_gpuFFT3dPlan(gpuFFT3dPlan* plan);                     /* gpu_fft0.h:56 */
 void gpuFFT3dPlan_forward(gpuFFT3dPlan* plan, float* input, float* output); /* gpu_fft0.h:64 */
 void gpuFFT3dPlan_inverse(gpuFFT3dPlan* plan, float* input, float* output); /* gpu_fft0.h:75 */
-int gpuFFT3dPlan_normalization(gpuFFT3dPlan* plan);               /* gpu_fft0.cu:197 */
+int gpuFFT3dPlan_normalization(gpuFFT3dPlan* plan);               /* gpu_fft0.cu:112-114 */
 
 /* ---- gpu_reduction.h ---- */
 #define REDUCE_ADD 1

@@ -6,14 +6,14 @@
  * (Sim.calcHeff -> Conv.Convolve -> gpuFFT3dPlan_forward x3 ->
  * gpu_kernelmul6/4 -> gpuFFT3dPlan_inverse x3 -> gpu_add_local_fields ->
  * gpu_deltaM -> gpu_madd / gpu_linear_combination -> gpu_normalize_uniform,
- * src/go/sim/field.go:427-433, conv.go:57-100, adaptive_heun.go:34-76,
+ * src/go/sim/field.go:74-80, conv.go:57-100, adaptive_heun.go:34-76,
  * rk.go:279-445) into a handful of kernels that keep the state on the
  * device.  Every function returns an MMX_* status and never aborts; every
  * launch goes to the caller's stream.
  *
  * Units and axes are the reference's internal ones: lengths in exchange
  * lengths sqrt(2A/(mu0 Ms^2)), time in 1/(gamma0 Ms), fields in mu0 Ms
- * (src/go/sim/material.go:338-366); arrays are [3][X][Y][Z] float32 with Z
+ * (src/go/sim/material.go:51-111); arrays are [3][X][Y][Z] float32 with Z
  * contiguous and internal X = the user's z axis (simgeom.go:19-38).
  */
 #ifndef MMX_H
@@ -72,7 +72,7 @@ typedef struct mmx_solver mmx_solver;
 const char* mmx_last_error(void);
 
 /* Builds a solver: allocates the state, computes the demag(+exchange)
- * kernel on the GPU (FaceKernel6, demag.go:127-185) and keeps its
+ * kernel on the GPU (FaceKernel6, demag.go:26-84) and keeps its
  * spectrum resident as one octant per component.  The magnetisation starts
  * at zero; set it with mmx_solver_set_m. */
 int mmx_solver_create(const mmx_params* p, mmx_solver** out);
@@ -90,7 +90,7 @@ int mmx_solver_normalize(mmx_solver* s, cudaStream_t stream);
 int mmx_solver_step(mmx_solver* s, int nsteps, cudaStream_t stream);
 
 /* Effective field h = demag + exchange + Zeeman + anisotropy of the device
- * array m (field.go:427-433); m and h are device arrays of 3*N floats. */
+ * array m (field.go:74-80); m and h are device arrays of 3*N floats. */
 int mmx_solver_field(mmx_solver* s, const float* m, float* h, cudaStream_t stream);
 
 /* <m>: the average magnetisation per internal component (the table output
@@ -127,6 +127,17 @@ int mmx_solver_energy(mmx_solver* s, double* energy, cudaStream_t stream);
 int mmx_solver_run(mmx_solver* s, double seconds, float period, float* rows, int max_rows, int* nrows,
                    long long max_steps, cudaStream_t stream);
 
+/* Sim.Relax (src/go/sim/relax.go:14-23): from this call on the RK steps
+ * compute the energy (at the FSAL stage, or the first stage of other
+ * tableaux, rk.go:321-337) and reject a trial whose energy rose
+ * (rk.go:297-301,425); the solver takes one step, then steps while the
+ * energy does not rise, at most max_steps steps.  *steps gets the steps
+ * taken and *energy the last energy (internal units, float32 as the
+ * reference keeps it).  RK solvers with the host dt controller only (the
+ * heun step computes no energy).  The energy stays wanted afterwards, as
+ * in the reference.  Synchronous. */
+int mmx_solver_relax(mmx_solver* s, long long max_steps, long long* steps, float* energy, cudaStream_t stream);
+
 /* Solver scalars: simulated time (internal units), current dt, the last
  * maximum torque and the last error estimate, steps taken. */
 int mmx_solver_state(mmx_solver* s, double* time, float* dt, float* max_torque, float* step_error, long long* steps);
@@ -148,9 +159,12 @@ int mmx_solver_use_graph(mmx_solver* s, int on);
  * state back to the host controller. */
 int mmx_solver_device_control(mmx_solver* s, int on);
 
-/* Per-pass timing with CUDA events on the step's stream: when on, each
- * kernel of the step is bracketed by events; mmx_solver_pass_times
- * returns the accumulated milliseconds and launch counts per pass name. */
+/* Per-pass timing with CUDA events on the step's stream; mmx_solver_pass_times
+ * returns the accumulated milliseconds and launch counts per pass name.
+ * on = 1: each kernel of a directly launched step is bracketed by events;
+ * on = 2 (fixed-step solvers): the step is replayed as a graph whose passes
+ * are bracketed by event-record nodes, so the times are those of the
+ * passes as the graph runs them (one host synchronisation per step). */
 int mmx_solver_profile(mmx_solver* s, int on);
 int mmx_solver_pass_times(mmx_solver* s, int max, char (*names)[32], double* ms, long long* launches, int* n);
 
@@ -258,17 +272,21 @@ int mmx_dft_tc(const float2* in, float2* out, int nvec, int inverse, cudaStream_
  * allocates nothing.  'input' (n floats) and 'result' (1 float) are device
  * pointers; the launch is asynchronous on 'stream'.  n is limited to
  * MMX_REDUCE_STATIC_MAX_N; larger n returns MMX_ERR_SIZE.  The first call
- * on a device looks up the array's device address (cudaGetSymbolAddress)
- * and should come before any stream capture.  Every call shares the array:
- * calls that overlap on the GPU race and must be serialised by the caller. */
+ * on a device (per CUDA context: again after a device reset) looks up the
+ * array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  While another thread captures a graph in global mode,
+ * pass a non-blocking stream of your own (cudaStreamNonBlocking): a launch
+ * on the legacy default stream would join the capture's implicit
+ * synchronisation and fail.  Every call shares the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
 #define MMX_REDUCE_STATIC_BLOCKS 1024
 #define MMX_REDUCE_STATIC_MAX_N (MMX_REDUCE_STATIC_BLOCKS * 4096)
 int mmx_reduce_static(int operation, const float* input, int n, float* result, cudaStream_t stream);
 
 /* FaceKernel6 on the GPU: the 6 real-space components (XX,YY,ZZ,YZ,XZ,XY)
  * of the padded grid P, written to k6 (device, 6*P0*P1*P2 floats),
- * bit-identical to src/go/sim/demag.go:127-185 in float32.  If exch6 != 0
- * the six-neighbour exchange stencil is added (exchange.go:328-353). */
+ * bit-identical to src/go/sim/demag.go:26-84 in float32.  If exch6 != 0
+ * the six-neighbour exchange stencil is added (exchange.go:44-71). */
 int mmx_face_kernel6(const int P[3], const int periodic[3], const float cellsize[3], int accuracy, int exch6,
                      float* k6, cudaStream_t stream);
 

@@ -65,7 +65,7 @@ int mmxd_steps(mmxd_sim* s, int n);           /* Sim.Steps (simrun.go:88-92) */
 int mmxd_run(mmxd_sim* s, double seconds);    /* Sim.Run step loop (simrun.go:19-57) */
 int mmxd_get_m(mmxd_sim* s, float* m);        /* 3N floats, internal order */
 int mmxd_set_m(mmxd_sim* s, const float* m);
-int mmxd_heff(mmxd_sim* s, const float* m, float* h); /* calcHeff (field.go:427-433), host arrays */
+int mmxd_heff(mmxd_sim* s, const float* m, float* h); /* calcHeff (field.go:74-80), host arrays */
 int mmxd_avg_m(mmxd_sim* s, float out[3]);    /* <m> per internal component (simoutput.go:236) */
 double mmxd_time(mmxd_sim* s);                /* internal units */
 float mmxd_dt(mmxd_sim* s);                   /* internal units */

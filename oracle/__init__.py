@@ -185,6 +185,19 @@ class OracleSim:
             raise RuntimeError("oracle: dt is NaN")
         return rows[:k]
 
+    def relax(self, max_steps=1000000):
+        """Sim.Relax (relax.go:14-23); returns the steps taken."""
+        f = _fn(self.bits, "sim_relax", ctypes.c_longlong)
+        f.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
+        k = f(ctypes.c_void_p(self.h), max_steps)
+        if k < 0:
+            raise RuntimeError("oracle: dt is NaN")
+        return k
+
+    def last_energy(self):
+        """Sim.energy: the total energy the last RK step computed."""
+        return _fn(self.bits, "sim_last_energy", ctypes.c_double)(ctypes.c_void_p(self.h))
+
     def step_error(self):
         rt = ctypes.c_float if self.bits == 32 else ctypes.c_double
         return _fn(self.bits, "sim_step_error", rt)(ctypes.c_void_p(self.h))

@@ -46,8 +46,8 @@
 typedef struct { double re, im; } cplx;
 
 /* ------------------------------------------------------------------ */
-/* Kernel generation: FaceKernel6 (src/go/sim/demag.go:127-185) and the  */
-/* point-charge face integral (demag.go:243-284).                        */
+/* Kernel generation: FaceKernel6 (src/go/sim/demag.go:26-84) and the  */
+/* point-charge face integral (demag.go:142-183).                        */
 /* ------------------------------------------------------------------ */
 
 /* Go's wrap (src/go/sim/kernel.go:62-72). */
@@ -67,7 +67,7 @@ static REAL vnorm(const REAL v[3]) {
 }
 
 /* faceIntegral: field at R of the two charged faces of a unit cell
- * magnetised along s, n x n point charges per face (demag.go:243-284). */
+ * magnetised along s, n x n point charges per face (demag.go:142-183). */
 static void face_integral(REAL B[3], const REAL R[3], const REAL cs[3], int s, int n) {
   int u = s, v = (s + 1) % 3, w = (s + 2) % 3;
   REAL surface = cs[v] * cs[w];
@@ -109,7 +109,7 @@ static void face_integral(REAL B[3], const REAL R[3], const REAL cs[3], int s, i
 static const int KIDX[3][3] = {{0, 5, 4}, {5, 1, 3}, {4, 3, 2}};
 
 /* FaceKernel6: k[6][PX][PY][PZ], accumulated over periodic images in loop
- * order, indices wrapped (demag.go:127-185). */
+ * order, indices wrapped (demag.go:26-84). */
 void FN(face_kernel6)(const int size[3], const REAL cellsize[3], int accuracy,
                       const int periodic[3], REAL* k) {
   int64_t n3 = (int64_t)size[0] * size[1] * size[2];
@@ -143,7 +143,7 @@ void FN(face_kernel6)(const int size[3], const REAL cellsize[3], int accuracy,
   }
 }
 
-/* Exch6NgbrKernel added into the diagonal components (exchange.go:328-353,
+/* Exch6NgbrKernel added into the diagonal components (exchange.go:44-71,
  * init.go:256-267); in 2D the +-x writes overwrite the centre. */
 void FN(add_exch6_kernel)(const int size[3], const REAL cellsize[3], REAL* k) {
   int64_t n3 = (int64_t)size[0] * size[1] * size[2];
@@ -247,7 +247,7 @@ static void fft_line(const fftplan* p, cplx* x, cplx* work, int sign) {
 }
 
 /* ------------------------------------------------------------------ */
-/* Padded convolution (src/go/sim/conv.go:57-100, gpu_fft0.cu:181-194,  */
+/* Padded convolution (src/go/sim/conv.go:57-100, gpu_fft0.cu:96-109,  */
 /* gpu_kernmul.cu:25-141) with the spectrum in REAL between stages.     */
 /* ------------------------------------------------------------------ */
 
@@ -616,6 +616,8 @@ typedef struct {
   REAL *m0, *mbackup, *m1est, *t0;
   REAL torque, step_error;
   int steps, error;
+  int want_energy;  /* Sim.wantEnergy (sim.go:109), set by Relax */
+  REAL energy;      /* Sim.energy: the last total energy computed */
 } osim_t;
 
 static void set_tableau(osim_t* s) {
@@ -684,7 +686,7 @@ static void set_tableau(osim_t* s) {
   }
 }
 
-/* Units (material.go:338-366) with float32 rounding at each operation in
+/* Units (material.go:51-111) with float32 rounding at each operation in
  * the FP32 build. */
 static void init_units(osim_t* s) {
   REAL mu0 = (REAL)(4.0e-7 * 3.14159265358979323846);
@@ -768,7 +770,7 @@ void FN(sim_free)(void* p) {
   free(s);
 }
 
-/* calcHeff (field.go:427-433): demag+exchange by convolution, then the
+/* calcHeff (field.go:74-80): demag+exchange by convolution, then the
  * local fields. */
 void FN(sim_heff)(void* p, const REAL* m, REAL* h) {
   osim_t* s = (osim_t*)p;
@@ -812,6 +814,8 @@ static void heun_step(osim_t* s) {
   }
 }
 
+void FN(sim_energy)(void* p, const REAL* m, REAL* out);
+
 /* RK.step (rk.go:279-445). */
 static void rk_step(osim_t* s) {
   int order = s->stages;
@@ -824,6 +828,9 @@ static void rk_step(osim_t* s) {
   int good = 0, trials = 0;
   const REAL maxErr = (REAL)s->cfg.maxerror;
   const REAL ut = s->T;
+  /* energy must not rise when it is wanted (rk.go:297-301,425) */
+  REAL prevEnergy = s->energy;
+  if (prevEnergy == 0) prevEnergy = (REAL)9999999999.;
   while (!good && trials < 10) {
     trials++;
     for (int i = 0; i < order; i++) {
@@ -834,6 +841,9 @@ static void rk_step(osim_t* s) {
         memcpy(m1, m, sizeof(REAL) * n3);
         for (int j = 0; j < order; j++)
           if (s->a[i][j] != 0) madd(m1, s->dt * s->a[i][j], s->k[j], n3);
+        /* calcHeffEnergy at the last stage (FSAL) or the first (rk.go:321-337) */
+        if (s->want_energy && ((s->fsal && i == order - 1) || (!s->fsal && i == 0)))
+          FN(sim_energy)(s, m1, &s->energy);
         FN(sim_heff)(s, m1, s->k[i]);
         FN(delta_m)(m1, s->k[i], s->n, s->alpha, dtg1);
         s->fsal_init = 1;
@@ -866,7 +876,7 @@ static void rk_step(osim_t* s) {
       if (factor < (REAL)0.01) factor = (REAL)0.01;
       s->dt = s->dt * factor;
       if (s->dt != s->dt) { s->error = 1; return; }
-      if (err > 2 * maxErr) {
+      if (err > 2 * maxErr || (s->want_energy && s->energy > prevEnergy)) {
         memcpy(m, s->mbackup, sizeof(REAL) * n3);
         good = 0;
         if (!s->cfg.faithful) s->fsal_init = 0;
@@ -1012,6 +1022,27 @@ int FN(sim_run_table)(void* p, double duration, float period, float* rows, int m
   return nrow;
 }
 
+/* Sim.Relax (relax.go:14-23): with the energy wanted, one step, then steps
+ * while the energy does not rise; the energies compared are the ones the
+ * RK steps compute (float32 in the FP32 build).  At most max_steps steps;
+ * returns the steps taken, or -1 on a NaN.  wantEnergy stays set, as in
+ * the reference. */
+long long FN(sim_relax)(void* p, long long max_steps) {
+  osim_t* s = (osim_t*)p;
+  s->want_energy = 1;
+  long long k = 0;
+  if (FN(sim_step)(p)) return -1;
+  k++;
+  REAL prevE = s->energy + 1;
+  while (s->energy <= prevE && k < max_steps) {
+    prevE = s->energy;
+    if (FN(sim_step)(p)) return -1;
+    k++;
+  }
+  return k;
+}
+double FN(sim_last_energy)(void* p) { return (double)((osim_t*)p)->energy; }
+
 REAL FN(sim_torque)(void* p) { return ((osim_t*)p)->torque; }
 REAL FN(sim_step_error)(void* p) { return ((osim_t*)p)->step_error; }
 
@@ -1034,7 +1065,7 @@ void FN(convolve_standalone)(const int N[3], const int periodic[3], const REAL c
 
 /* Reference-layout forward transform of a real (N0,N1,N2) array padded to
  * (P0,P1,P2): output (P0,P1,P2+2) floats, interleaved half spectrum, as
- * gpuFFT3dPlan_forward leaves it (gpu_fft0.cu:181-186). */
+ * gpuFFT3dPlan_forward leaves it (gpu_fft0.cu:96-101). */
 void FN(fft_forward_padded)(const int N[3], const int P[3], const REAL* in, REAL* out) {
   conv_t c;
   memset(&c, 0, sizeof(c));
@@ -1049,7 +1080,7 @@ void FN(fft_forward_padded)(const int N[3], const int P[3], const REAL* in, REAL
 }
 
 /* Reference-layout inverse: (P0,P1,P2+2) half spectrum -> real (N0,N1,N2),
- * unnormalised (gpu_fft0.cu:190-194). */
+ * unnormalised (gpu_fft0.cu:105-109). */
 void FN(fft_inverse_padded)(const int N[3], const int P[3], const REAL* in, REAL* out) {
   conv_t c;
   memset(&c, 0, sizeof(c));

@@ -56,7 +56,7 @@ def test_face_kernel_self_term_cube():
 
 def test_face_kernel_2d_exchange_centre_overwrite():
     """In 2D (P0 = 1) the +-x exchange writes overwrite the centre value
-    (exchange.go:342-349): centre = demag + 1/hx."""
+    (exchange.go:58-65): centre = demag + 1/hx."""
     Pd = (1, 8, 8)
     cs = np.array([0.5, 0.7, 0.7], np.float32)
     k = O.face_kernel6(Pd, cs)

@@ -28,7 +28,7 @@ KERNEL_CASES = [
 @pytest.mark.parametrize("N,cs,per", KERNEL_CASES)
 def test_face_kernel_bitexact(eng, cuda, N, cs, per):
     """GPU FaceKernel6 + Exch6 == the oracle's float32 restatement of
-    demag.go:127-185 / exchange.go:328-353, bit for bit."""
+    demag.go:26-84 / exchange.go:44-71, bit for bit."""
     Pd = tuple(2 * n if (n > 1 and p == 0) else n for n, p in zip(N, per))
     csf = np.array(cs, np.float32)
     ref = O.face_kernel6(Pd, csf, periodic=per)

@@ -53,3 +53,50 @@ def test_reduce_static_rejects_oversize(eng, cuda):
     rc = L.mmx_reduce_static(1, ctypes.c_void_p(a.data_ptr()), 4_194_305, ctypes.c_void_p(out.data_ptr()), None)
     assert rc == 3  # MMX_ERR_SIZE, nothing launched
     assert b"MMX_REDUCE_STATIC_MAX_N" in L.mmx_last_error()
+
+
+def test_reduce_static_beside_a_global_mode_capture(eng, cuda):
+    """The case the entry point exists for: while one thread captures a CUDA
+    graph in global mode (where cudaMalloc from any thread is an error),
+    another thread reduces on a non-blocking stream of its own.  The first
+    call, which looks the array's address up, comes before the capture."""
+    import threading
+
+    L = eng.lib()
+    n = 100_003
+    a = cuda.from_numpy(np.random.default_rng(12).standard_normal(n).astype(np.float32)).cuda()
+    out = cuda.zeros(1, device="cuda")
+    assert L.mmx_reduce_static(1, ctypes.c_void_p(a.data_ptr()), n, ctypes.c_void_p(out.data_ptr()), None) == 0
+    cuda.cuda.synchronize()
+    want = {op: reference_reduce(L, cuda, op, a, n) for op in OPS}
+    side = cuda.cuda.Stream()  # torch streams are created non-blocking
+    results = cuda.zeros(len(OPS), device="cuda")
+    started, reduced = threading.Event(), threading.Event()
+    rcs = []
+
+    def reducer():
+        started.wait(30)
+        for k, op in enumerate(OPS):
+            rcs.append(L.mmx_reduce_static(op, ctypes.c_void_p(a.data_ptr()), n,
+                                           ctypes.c_void_p(results.data_ptr() + 4 * k),
+                                           ctypes.c_void_p(side.cuda_stream)))
+        reduced.set()
+
+    t = threading.Thread(target=reducer)
+    t.start()
+    g = cuda.cuda.CUDAGraph()
+    x = cuda.zeros(16, device="cuda")
+    with cuda.cuda.graph(g, capture_error_mode="global"):
+        x.add_(1.0)
+        started.set()
+        assert reduced.wait(30)
+    t.join(30)
+    side.synchronize()
+    g.replay()
+    cuda.cuda.synchronize()
+    assert rcs == [0] * len(OPS), [L.mmx_last_error()]
+    got = results.cpu().numpy()
+    for k, op in enumerate(OPS):
+        tol = 1e-6 * max(1.0, abs(want[op])) if op in (1, 5) else 0.0
+        assert abs(float(got[k]) - want[op]) <= tol, (OPS[op], got[k], want[op])
+    assert float(x[0].item()) == 1.0

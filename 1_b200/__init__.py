@@ -68,6 +68,8 @@ class MmxParams(ctypes.Structure):
         ("faithful", ctypes.c_int),
         ("accuracy", ctypes.c_int),
         ("precision", ctypes.c_int),
+        ("thermal_k", ctypes.c_float),
+        ("thermal_seed", ctypes.c_uint),
     ]
 
 
@@ -258,6 +260,10 @@ MMX = {
     "mmx_server_clock": (ctypes.c_double, [ctypes.c_void_p]),
     "mmx_server_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t),
                                         ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
+    "mmx_write_ovf": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, c_int_p, ctypes.POINTER(ctypes.c_double),
+                                     ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double]),
+    "mmx_write_odt": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p]),
     "mmx_dft_tc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "mmx_reduce_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                          ctypes.c_void_p]),
@@ -350,8 +356,19 @@ def units(msat, aexch):
     return dict(length=L, time=T, field=B, edens=E)
 
 
+def thermal_k(msat, aexch, alpha, cell, temperature):
+    """sigma^2 dt (internal units) of the thermal field at 'temperature'
+    kelvin: sigma = sqrt(2 alpha kB T / (gamma0 mu0 Ms V dt_SI)) / Ms
+    (src/go/sim/temperature.go:27-36), dt_SI = dt * unit time."""
+    u = units(msat, aexch)
+    kB, gamma0, mu0 = 1.380650424e-23, 2.211e5, 4.0e-7 * np.pi
+    V = float(cell[0]) * float(cell[1]) * float(cell[2])
+    return float(2.0 * alpha * kB * temperature / (gamma0 * mu0 * msat * V * float(u["time"])) / (msat * msat))
+
+
 def mmx_params(grid, cell, msat, aexch, alpha, bext=(0, 0, 0), solver="heun", dt=0.0, maxerror=0.0, anis=0,
-               k1=0.0, axis=(0, 0, 1), periodic=(0, 0, 0), faithful=1, exch_type=6, precision=0):
+               k1=0.0, axis=(0, 0, 1), periodic=(0, 0, 0), faithful=1, exch_type=6, precision=0, temperature=0.0,
+               thermal_seed=0):
     """Builds mmx_params from the reference's user-level (SI, user x,y,z)
     inputs with the same float32 conversions as the Go driver."""
     u = units(msat, aexch)
@@ -377,6 +394,8 @@ def mmx_params(grid, cell, msat, aexch, alpha, bext=(0, 0, 0), solver="heun", dt
     p.faithful = faithful
     p.accuracy = 8
     p.precision = precision
+    p.thermal_k = thermal_k(msat, aexch, alpha, cell, temperature) if temperature else 0.0
+    p.thermal_seed = thermal_seed
     return p
 
 
@@ -569,6 +588,23 @@ def batch_config(count, seed=4, cell=3e-9, solver="rk4", dt=5e-15):
         out.append(dict(grid=(nx, ny, nz), cell=(cell, cell, cell), msat=ms, aexch=a, alpha=alpha,
                         bext=tuple(float(x) for x in bmag * d), solver=solver, dt=dt))
     return out
+
+
+def write_ovf(path, m, cell, version=2, binary=True, valueunit="A/m", multiplier=1.0, stage_time=0.0,
+              total_time=0.0):
+    """Writes m ([3][X][Y][Z], internal order) as an OVF file; cell is the
+    internal (X, Y, Z) cell size in metres (mmx_write_ovf)."""
+    a = np.ascontiguousarray(m, dtype=np.float32)
+    size = (ctypes.c_int * 3)(*a.shape[1:])
+    cs = (ctypes.c_double * 3)(*[float(c) for c in cell])
+    _check(lib().mmx_write_ovf(os.fsencode(path), a.ctypes.data, size, cs, version, 1 if binary else 0,
+                               valueunit.encode(), multiplier, stage_time, total_time))
+
+
+def write_odt(path, rows, title="mumax data"):
+    """Writes table rows of Solver.run as an ODT 1.0 file (mmx_write_odt)."""
+    r = np.ascontiguousarray(rows, dtype=np.float32).reshape(-1, 7)
+    _check(lib().mmx_write_odt(os.fsencode(path), r.ctypes.data, r.shape[0], title.encode()))
 
 
 # --------------------------------------------------------------------------

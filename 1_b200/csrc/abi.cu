@@ -25,6 +25,7 @@
 //    (gpu_linalg.cu:103-112 reads before the bounds check);
 //  * gpu_gaussian_noise uses a counter-based Philox generator of its own
 //    (reference: cuRAND default generator, gpu_temperature.cu:34-41).
+#include "fft_generic.cuh"
 #include <assert.h>
 #include <math.h>
 #include <string.h>
@@ -605,6 +606,11 @@ void gpu_copy_unpad2D(float* source, float* dest, int S1, int S2, int D1, int D2
 // ---------------------------------------------------------------------
 // FFT plan (gpu_fft0.cu:33-109) on the engine's zero-aware passes
 // ---------------------------------------------------------------------
+struct PlanEngine {
+  int generic = 0;
+  BoxPlan box;
+  GenericPlan gen;
+};
 gpuFFT3dPlan* new_gpuFFT3dPlan_padded(int* size, int* paddedSize) {
   ABI_ASSERT(paddedSize[0] > 0 && paddedSize[1] > 1 && paddedSize[2] > 1, "new_gpuFFT3dPlan_padded");
   gpuFFT3dPlan* plan = (gpuFFT3dPlan*)calloc(1, sizeof(gpuFFT3dPlan));
@@ -616,29 +622,42 @@ gpuFFT3dPlan* new_gpuFFT3dPlan_padded(int* size, int* paddedSize) {
   }
   plan->paddedN = paddedSize[0] * paddedSize[1] * paddedSize[2];
   plan->paddedComplexN = paddedSize[0] * paddedSize[1] * (paddedSize[2] + 2);
-  BoxPlan* bp = new BoxPlan();
-  int rc = box_plan_init(bp, size, paddedSize);
+  // sizes whose factors are 2, 3, 5, 7 (even padded Z): the zero-aware
+  // passes; any other size (cufftPlan3d takes every size): the generic
+  // complex-box path with Bluestein lines (fft_generic.cu)
+  PlanEngine* pe = new PlanEngine();
+  int rc = box_plan_init(&pe->box, size, paddedSize);
+  if (rc != MMX_OK && generic_plan_needed(size, paddedSize)) {
+    pe->generic = 1;
+    rc = generic_plan_init(&pe->gen, size, paddedSize);
+  }
   MMX_ABORT_ON(rc != MMX_OK,
-               "unsupported FFT size %dx%dx%d padded to %dx%dx%d (padded Z must be even; every padded size a "
-               "product of 2,3,5,7 and <= 16384)",
+               "unsupported FFT size %dx%dx%d padded to %dx%dx%d (padded sizes with a prime factor above 7 up "
+               "to 4096, others up to 8192)",
                size[0], size[1], size[2], paddedSize[0], paddedSize[1], paddedSize[2]);
-  plan->engine = bp;
+  plan->engine = pe;
   return plan;
 }
 gpuFFT3dPlan* new_gpuFFT3dPlan(int* size) { return new_gpuFFT3dPlan_padded(size, size); }
 void delete_gpuFFT3dPlan(gpuFFT3dPlan* plan) {
   if (!plan) return;
-  delete (BoxPlan*)plan->engine;
+  PlanEngine* pe = (PlanEngine*)plan->engine;
+  if (pe && pe->generic) generic_plan_free(&pe->gen);
+  delete pe;
   free(plan->size);
   free(plan->paddedSize);
   free(plan);
 }
 void gpuFFT3dPlan_forward(gpuFFT3dPlan* plan, float* input, float* output) {
-  GK_CHECK(box_forward((BoxPlan*)plan->engine, input, (float2*)output, 0));
+  PlanEngine* pe = (PlanEngine*)plan->engine;
+  if (pe->generic) GK_CHECK(generic_forward(&pe->gen, input, output, 0));
+  else GK_CHECK(box_forward(&pe->box, input, (float2*)output, 0));
   GK_SYNC();
 }
 void gpuFFT3dPlan_inverse(gpuFFT3dPlan* plan, float* input, float* output) {
-  GK_CHECK(box_inverse((BoxPlan*)plan->engine, (float2*)input, output, 0));
+  PlanEngine* pe = (PlanEngine*)plan->engine;
+  if (pe->generic) GK_CHECK(generic_inverse(&pe->gen, input, output, 0));
+  else GK_CHECK(box_inverse(&pe->box, (float2*)input, output, 0));
   GK_SYNC();
 }
 int gpuFFT3dPlan_normalization(gpuFFT3dPlan* plan) {
@@ -1016,24 +1035,11 @@ void gpu_directionial_diff(float ux, float uy, float uz, float* in, float* out, 
 // SC'11) and the Box-Muller transform; the counter advances per call so
 // successive calls give fresh numbers.
 // ---------------------------------------------------------------------
-__device__ __forceinline__ uint4 philox_round(uint4 c, uint2 k) {
-  unsigned int hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
-  unsigned int hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
-  return make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
-}
-__device__ uint4 philox10(uint4 c, uint2 k) {
-  for (int r = 0; r < 10; r++) {
-    c = philox_round(c, k);
-    k.x += 0x9E3779B9u;
-    k.y += 0xBB67AE85u;
-  }
-  return c;
-}
 __global__ void k_gauss(float* out, float mean, float sd, int64_t n, unsigned long long seed, unsigned long long ctr) {
   int64_t pairs = (n + 1) / 2;
   GRID_STRIDE(p, pairs) {
     uint4 c = make_uint4((unsigned)p, (unsigned)(p >> 32), (unsigned)ctr, (unsigned)(ctr >> 32));
-    uint4 r = philox10(c, make_uint2((unsigned)seed, (unsigned)(seed >> 32)));
+    uint4 r = philox4x32_10(c, make_uint2((unsigned)seed, (unsigned)(seed >> 32)));
     float u1 = ((float)(r.x >> 8) + 1.f) * (1.f / 16777216.f);  // (0, 1]
     float u2 = (float)(r.y >> 8) * (1.f / 16777216.f);
     float rad = sqrtf(-2.f * logf(u1));

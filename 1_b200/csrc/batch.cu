@@ -628,6 +628,10 @@ static int batch_check(mmx_solver* s, int solver) {
     mmx_set_error("batched form: FP32 transforms only (precision = 0)");
     return MMX_ERR_ARG;
   }
+  if (s->p.thermal_k != 0.f) {
+    mmx_set_error("batched form: no thermal field (its noise is drawn per step on the host controller)");
+    return MMX_ERR_ARG;
+  }
   if (s->p.solver != solver || s->p.max_error != 0.f) {
     mmx_set_error("all instances of a batch must use the same fixed-step solver (Heun or RK4)");
     return MMX_ERR_ARG;

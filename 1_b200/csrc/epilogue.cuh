@@ -96,6 +96,14 @@ __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float 
         float s = FA(FA(FM(mx, FA(hx, ea.lf.hext[0])), FM(my, FA(hy, ea.lf.hext[1]))), FM(mz, FA(hz, ea.lf.hext[2])));
         *eacc += (double)FM(-0.5f, s);
       }
+      // the thermal field, added after the energy density (field.go:64-80)
+      if (ea.lf.sigma != 0.f) {
+        float nrm[3];
+        thermal_normals(ea.lf, g, nrm);
+        hx = FA(hx, FM(ea.lf.sigma, nrm[0]));
+        hy = FA(hy, FM(ea.lf.sigma, nrm[1]));
+        hz = FA(hz, FM(ea.lf.sigma, nrm[2]));
+      }
     }
     if (MODE == EPI_FIELD) {
       ea.out0[g] = hx;

@@ -4,6 +4,7 @@
 // same values as the corresponding sequence of primitive calls.
 #pragma once
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #define FM(a, b) __fmul_rn((a), (b))
 #define FA(a, b) __fadd_rn((a), (b))
@@ -39,7 +40,46 @@ struct LocalField {
   int anis;     // 0 none, 1 uniaxial
   float K;
   float u[3];
+  // thermal field (RK stages): h += sigma * N(0,1) per cell and component,
+  // the same numbers for every stage of a step (rk.go:289-292); 0 = off
+  float sigma;
+  unsigned int seed, step_lo, step_hi;
 };
+
+// Philox-4x32-10 (J. Salmon, M. Moraes, R. Dror, D. Shaw, "Parallel random
+// numbers: as easy as 1, 2, 3", SC'11): counter c, key k
+__host__ __device__ __forceinline__ unsigned int philox_mulhi(unsigned int a, unsigned int b) {
+  return (unsigned int)(((unsigned long long)a * b) >> 32);
+}
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    unsigned int hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    unsigned int hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// three standard normals of cell g at step (lo, hi): one Philox block,
+// two Box-Muller pairs (u1 in (0, 1], u2 in [0, 1))
+__device__ __forceinline__ void thermal_normals(const LocalField& lf, int64_t g, float* nrm) {
+  uint4 r = philox4x32_10(make_uint4((unsigned int)g, (unsigned int)((uint64_t)g >> 32), lf.step_lo, lf.step_hi),
+                          make_uint2(lf.seed, 0x4D4D5854u));
+  float u1 = ((float)(r.x >> 8) + 1.f) * (1.f / 16777216.f);
+  float u2 = (float)(r.y >> 8) * (1.f / 16777216.f);
+  float u3 = ((float)(r.z >> 8) + 1.f) * (1.f / 16777216.f);
+  float u4 = (float)(r.w >> 8) * (1.f / 16777216.f);
+  float a = sqrtf(-2.f * logf(u1)), b = sqrtf(-2.f * logf(u3));
+  float s1, c1, s2, c2;
+  sincospif(2.f * u2, &s1, &c1);
+  sincospif(2.f * u4, &s2, &c2);
+  nrm[0] = a * c1;
+  nrm[1] = a * s1;
+  nrm[2] = b * c2;
+}
 
 // gpu_add_local_fields, uniform Hext, ANIS_NONE / ANIS_UNIAXIAL
 // (gpu_local_contr3.cu:21-36,133-143).

@@ -665,6 +665,12 @@ static cudaError_t rk_stage(mmx_solver* s, int i, cudaStream_t st, float* dt_dev
   ea.dt_dev = dt_dev;
   for (int j = 0; j < s->stages; j++) ea.kbuf[j] = s->kb[j];
   ea.stage = i;
+  if (s->noise_sigma != 0.f) {
+    ea.lf.sigma = s->noise_sigma;
+    ea.lf.seed = s->p.thermal_seed;
+    ea.lf.step_lo = (unsigned int)s->noise_step;
+    ea.lf.step_hi = (unsigned int)((unsigned long long)s->noise_step >> 32);
+  }
   // calcHeffEnergy at the last stage (FSAL) or the first (rk.go:321-337)
   if (s->want_energy && s->eacc && (s->fsal ? i == s->stages - 1 : i == 0)) ea.energy = s->eacc;
   if (i == s->stages - 1) {
@@ -752,6 +758,11 @@ static int rk_step(mmx_solver* s, cudaStream_t st) {
   int good = 0, trials = 0;
   const bool want_e = s->want_energy && s->eacc;
   const int e_stage = s->fsal ? s->stages - 1 : 0;
+  // the thermal noise, fixed for the step's trials (updateTempNoise at the
+  // step start, rk.go:289-292; temperature.go:27-36)
+  const bool thermal = s->p.thermal_k != 0.f;
+  s->noise_sigma = thermal ? (float)sqrt((double)f32_div(s->p.thermal_k, s->dt)) : 0.f;
+  s->noise_step = s->steps;
   // energy must not rise when it is wanted (rk.go:297-301,425)
   float prevE = s->energy;
   if (prevE == 0.f) prevE = 9999999999.f;
@@ -780,8 +791,9 @@ static int rk_step(mmx_solver* s, cudaStream_t st) {
         if (e != cudaSuccess) { mmx_set_error(cudaGetErrorString(e)); return MMX_ERR_CUDA; }
         s->fsal_init = 1;
       }
-      if (i == 0 && bounds) {
-        // dt bounds from the maximum torque (rk.go:348-373)
+      if (i == 0 && bounds && !thermal) {
+        // dt bounds from the maximum torque (rk.go:348-373; not with a
+        // thermal field)
         float mt = 0;
         MMX_TRY(cudaMemcpyAsync(&mt, s->scratch + 1, sizeof(float), cudaMemcpyDeviceToHost, st));
         MMX_TRY(cudaStreamSynchronize(st));
@@ -932,6 +944,11 @@ extern "C" int mmx_solver_create(const mmx_params* p, mmx_solver** out) {
   s->CS = (int64_t)s->N[0] * s->P[1] * s->HZ;
   set_tableau(s);
   if (p->solver != MMX_SOLVER_HEUN && s->stages == 0) { delete s; mmx_set_error("unknown solver"); return MMX_ERR_ARG; }
+  if (p->thermal_k != 0.f && (p->solver == MMX_SOLVER_HEUN || p->thermal_k < 0.f || p->precision)) {
+    delete s;
+    mmx_set_error("thermal field: RK solvers with the FP32 transforms only (the reference runs it with rk12)");
+    return MMX_ERR_ARG;
+  }
   s->dt = p->dt;
   size_t n3 = 3 * (size_t)s->n;
 #define ALLOC(ptr, bytes)                                                   \
@@ -1220,6 +1237,10 @@ extern "C" int mmx_solver_device_control(mmx_solver* s, int on) {
     mmx_set_error("device control: adaptive RK solvers (rk12, rk23, rkck, rkdp) only");
     return MMX_ERR_ARG;
   }
+  if (on && s->p.thermal_k != 0.f) {
+    mmx_set_error("device control: not with a thermal field (its noise is drawn per step on the host controller)");
+    return MMX_ERR_ARG;
+  }
   if (on && !s->devctl) {
     if (!s->rkdev && cudaMalloc(&s->rkdev, sizeof(RkDev)) != cudaSuccess) {
       mmx_set_error("out of device memory");
@@ -1348,7 +1369,8 @@ static int profiled_graph_steps(mmx_solver* s, int nsteps, cudaStream_t st) {
 extern "C" int mmx_solver_step(mmx_solver* s, int nsteps, cudaStream_t st) {
   if (!s || nsteps < 0) { mmx_set_error("bad argument"); return MMX_ERR_ARG; }
   if (s->devctl) return rk_device_steps(s, nsteps, st);
-  const bool fixed_graphable = (s->p.solver == MMX_SOLVER_HEUN && s->p.max_error == 0.f) || rk_fixed(s);
+  const bool fixed_graphable =
+      ((s->p.solver == MMX_SOLVER_HEUN && s->p.max_error == 0.f) || rk_fixed(s)) && s->p.thermal_k == 0.f;
   if (s->profile == 2 && fixed_graphable && !s->want_energy) {
     if (s->p.solver != MMX_SOLVER_HEUN && s->dt_uploaded != s->dt) {
       float v[2] = {s->dt, 0.f};

@@ -72,6 +72,8 @@ struct mmx_solver {
   cudaGraphExec_t rungraph = nullptr;     // devctl: WHILE-conditional run graph
   cudaStream_t rungraph_stream = nullptr;
   double* eacc = nullptr;                 // energy accumulator (one double)
+  float noise_sigma = 0.f;                // thermal field of the current step (0: off)
+  long long noise_step = 0;               // its step number (the noise counter)
   int want_energy = 0;                    // Sim.wantEnergy: RK steps compute the energy (Relax)
   float energy = 0.f;                     // Sim.energy: the last energy an RK step computed
   // profiling: 1 = events around each launch of directly launched steps;

@@ -64,6 +64,14 @@ typedef struct mmx_params {
   int accuracy;         /* face-integral points per side (reference: 8) */
   int precision;        /* 0: FP32 transforms; 1: split-BF16 tensor-core DFT
                            GEMMs for the Y convolution (2D films, Ny = 512) */
+  float thermal_k;      /* thermal field (temperature.go:21-36): each RK step adds
+                           sigma N(0,1) per cell and component to the field of
+                           all its stages, sigma = sqrt(thermal_k / dt) with
+                           thermal_k = 2 alpha kB T / (gamma0 mu0 Ms V T_unit Ms^2)
+                           (V the cell volume in m^3, T_unit the time unit);
+                           0 = off.  RK solvers, host dt controller only */
+  unsigned int thermal_seed; /* noise stream: Philox-4x32-10 keyed by the seed,
+                           counted by (cell, step) */
 } mmx_params;
 
 typedef struct mmx_solver mmx_solver;
@@ -137,6 +145,20 @@ int mmx_solver_run(mmx_solver* s, double seconds, float period, float* rows, int
  * heun step computes no energy).  The energy stays wanted afterwards, as
  * in the reference.  Synchronous. */
 int mmx_solver_relax(mmx_solver* s, long long max_steps, long long* steps, float* energy, cudaStream_t stream);
+
+/* Output formats of the reference's omf package, for a [3][X][Y][Z] host
+ * array m of internal size 'size' with internal cell size 'cellsize' in
+ * metres: an OVF 1.0 ("rectangular mesh v1.0", Binary 4 big-endian) or
+ * OVF 2.0 (Binary 4 little-endian) file, or text with binary = 0, in user
+ * axes x, y, z = internal Z, Y, X (src/go/mumax/omf/output.go:41-260).
+ * valueunit / valuemultiplier as the reference writes them (e.g. "A/m" and
+ * Ms for m); stage_time / total_time go to the OVF 2.0 header. */
+int mmx_write_ovf(const char* path, const float* m, const int size[3], const double cellsize[3], int ovf_version,
+                  int binary, const char* valueunit, double valuemultiplier, double stage_time, double total_time);
+/* ODT 1.0 data table (omf/odt.go:103-131) of rows from mmx_solver_run:
+ * columns Time, Mx/Ms, My/Ms, Mz/Ms, max_dm/dt, min_Mz/Ms, max_Mz/Ms
+ * (simoutput.go:161-208). */
+int mmx_write_odt(const char* path, const float* rows, int nrows, const char* title);
 
 /* Solver scalars: simulated time (internal units), current dt, the last
  * maximum torque and the last error estimate, steps taken. */

@@ -42,6 +42,8 @@ class OCfg(ctypes.Structure):
         ("faithful", ctypes.c_int),
         ("accuracy", ctypes.c_int),
         ("maxthreads", ctypes.c_int),
+        ("temperature", ctypes.c_double),
+        ("thermal_seed", ctypes.c_int),
     ]
 
 
@@ -79,7 +81,7 @@ def _fn(bits, name, restype=None):
 
 def make_cfg(grid, cell, msat, aexch, alpha, bext=(0, 0, 0), solver="heun", dt=0.0, maxerror=0.0,
              anis=0, k1=0.0, axis=(0, 0, 1), periodic=(0, 0, 0), faithful=1, exch_type=6,
-             mindm=0.0, maxdm=0.0, mindt=0.0, maxdt=0.0, maxthreads=1024):
+             mindm=0.0, maxdm=0.0, mindt=0.0, maxdt=0.0, maxthreads=1024, temperature=0.0, thermal_seed=0):
     c = OCfg()
     c.grid[:] = list(grid)
     c.cell[:] = list(cell)
@@ -92,6 +94,7 @@ def make_cfg(grid, cell, msat, aexch, alpha, bext=(0, 0, 0), solver="heun", dt=0
     c.dt, c.maxerror = dt, maxerror
     c.mindm, c.maxdm, c.mindt, c.maxdt = mindm, maxdm, mindt, maxdt
     c.exch_type, c.faithful, c.accuracy, c.maxthreads = exch_type, faithful, 8, maxthreads
+    c.temperature, c.thermal_seed = temperature, thermal_seed
     return c
 
 

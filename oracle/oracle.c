@@ -594,6 +594,8 @@ typedef struct {
   int faithful;      /* 1 = keep the FSAL-after-reject quirk */
   int accuracy;      /* face-integral points per side (8) */
   int maxthreads;    /* device maxThreadsPerBlock, sets the sum order */
+  double temperature; /* K; 0 = no thermal field */
+  int thermal_seed;
 } ocfg_t;
 
 typedef struct {
@@ -618,6 +620,8 @@ typedef struct {
   int steps, error;
   int want_energy;  /* Sim.wantEnergy (sim.go:109), set by Relax */
   REAL energy;      /* Sim.energy: the last total energy computed */
+  REAL thermal_k;   /* sigma^2 dt of the thermal field (internal units) */
+  REAL* noise;      /* the thermal field of the current step (Sim.tempNoise) */
 } osim_t;
 
 static void set_tableau(osim_t* s) {
@@ -756,6 +760,14 @@ void* FN(sim_new)(const ocfg_t* cfg, const REAL* m_internal) {
     s->m0 = (REAL*)calloc(3 * s->n, sizeof(REAL));
     s->mbackup = (REAL*)calloc(3 * s->n, sizeof(REAL));
   }
+  /* thermal field: sigma^2 dt = 2 alpha kB T / (gamma0 mu0 Ms V T_unit) / Ms^2 */
+  if (cfg->temperature != 0) {
+    double V = cfg->cell[0] * cfg->cell[1] * cfg->cell[2];
+    double kB = 1.380650424e-23, g0 = 2.211e5, mu0 = 4.0e-7 * 3.14159265358979323846;
+    s->thermal_k = (REAL)(2.0 * cfg->alpha * kB * cfg->temperature / (g0 * mu0 * cfg->msat * V * (double)s->T) /
+                          (cfg->msat * cfg->msat));
+    s->noise = (REAL*)calloc(3 * s->n, sizeof(REAL));
+  }
   /* Sim.Run normalises m before stepping (simrun.go:24) */
   FN(normalize)(s->m, s->n);
   return s;
@@ -767,6 +779,7 @@ void FN(sim_free)(void* p) {
   free(s->m); free(s->h);
   for (int i = 1; i < 7; i++) free(s->k[i]);
   free(s->m0); free(s->mbackup); free(s->m1est); free(s->t0);
+  free(s->noise);
   free(s);
 }
 
@@ -776,6 +789,35 @@ void FN(sim_heff)(void* p, const REAL* m, REAL* h) {
   osim_t* s = (osim_t*)p;
   convolve(&s->conv, m, h);
   FN(add_local_fields)(m, h, s->n, s->hext, s->cfg.anis, s->K, s->u);
+  /* addThermalField (field.go:74-80, temperature.go:19-22) */
+  if (s->noise)
+    for (int64_t i = 0; i < 3 * s->n; i++) h[i] = h[i] + s->noise[i];
+}
+
+/* Philox-4x32-10 (Salmon et al., SC'11) and two Box-Muller pairs per cell:
+ * the engine's thermal-noise stream, restated (counter = cell, step; key =
+ * seed and a fixed word). */
+static void philox10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; r++) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c[0], p1 = (uint64_t)0xCD9E8D57u * c[2];
+    uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0, n1 = (uint32_t)p1, n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1,
+             n3 = (uint32_t)p0;
+    c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+static void thermal_noise(osim_t* s, REAL sigma, long long step) {
+  for (int64_t g = 0; g < s->n; g++) {
+    uint32_t c[4] = {(uint32_t)g, (uint32_t)((uint64_t)g >> 32), (uint32_t)step, (uint32_t)((uint64_t)step >> 32)};
+    philox10(c, (uint32_t)s->cfg.thermal_seed, 0x4D4D5854u);
+    double u1 = ((double)(c[0] >> 8) + 1.0) / 16777216.0, u2 = (double)(c[1] >> 8) / 16777216.0;
+    double u3 = ((double)(c[2] >> 8) + 1.0) / 16777216.0, u4 = (double)(c[3] >> 8) / 16777216.0;
+    double a = sqrt(-2.0 * log(u1)), b = sqrt(-2.0 * log(u3));
+    s->noise[g] = sigma * (REAL)(a * cos(2.0 * M_PI * u2));
+    s->noise[s->n + g] = sigma * (REAL)(a * sin(2.0 * M_PI * u2));
+    s->noise[2 * s->n + g] = sigma * (REAL)(b * cos(2.0 * M_PI * u4));
+  }
 }
 
 static void madd(REAL* a, REAL c, const REAL* b, int64_t n) {
@@ -828,6 +870,9 @@ static void rk_step(osim_t* s) {
   int good = 0, trials = 0;
   const REAL maxErr = (REAL)s->cfg.maxerror;
   const REAL ut = s->T;
+  /* the thermal noise of this step (rk.go:289-292, temperature.go:27-36) */
+  const int thermal = s->noise != NULL;
+  if (thermal) thermal_noise(s, (REAL)sqrt((double)(s->thermal_k / s->dt)), s->steps);
   /* energy must not rise when it is wanted (rk.go:297-301,425) */
   REAL prevEnergy = s->energy;
   if (prevEnergy == 0) prevEnergy = (REAL)9999999999.;
@@ -848,7 +893,7 @@ static void rk_step(osim_t* s) {
         FN(delta_m)(m1, s->k[i], s->n, s->alpha, dtg1);
         s->fsal_init = 1;
       }
-      if (i == 0) {
+      if (i == 0 && !thermal) {
         REAL maxT = FN(maxabs)(s->k[0], n3);
         s->torque = maxT;
         REAL dm = s->dt * maxT;

@@ -256,3 +256,37 @@ def test_memory_and_properties(L, cuda):
     L.free_gpu_array(p)
     assert L.gpu_maxthreads() >= 256
     assert L.gpu_stride_float() >= 1
+
+
+GENERIC_SIZES = [((3, 11, 13), (6, 22, 26)), ((1, 17, 19), (1, 34, 38)), ((2, 5, 23), (4, 10, 46)),
+                 ((4, 7, 11), (4, 14, 22)), ((1, 6, 9), (1, 12, 9)), ((2, 3, 4), (2, 3, 4))]
+
+
+@pytest.mark.parametrize("N,Pd", GENERIC_SIZES)
+def test_fft_plan_any_size_vs_numpy(L, cuda, N, Pd):
+    """gpuFFT3dPlan_* for padded sizes with prime factors above 7 (and an
+    odd padded Z): the plan takes the generic path (Bluestein lines) where
+    cufftPlan3d takes any size (gpu_fft0.cu:57-68).  Forward against numpy's
+    real FFT in float64 (the reference's (P0,P1,P2+2)-float rows), inverse
+    as the unnormalised complex-to-real transform."""
+    n = int(np.prod(N))
+    a = np.random.default_rng(40).standard_normal(N).astype(np.float32)
+    box = np.zeros(Pd)
+    box[:N[0], :N[1], :N[2]] = a
+    want = np.fft.rfftn(box)
+    H = Pd[2] // 2 + 1
+    plan = L.new_gpuFFT3dPlan_padded(ints(*N), ints(*Pd))
+    din = dev(cuda, a)
+    spec = cuda.zeros(Pd[0] * Pd[1] * (Pd[2] + 2), device="cuda")
+    L.gpuFFT3dPlan_forward(plan, P(din), P(spec))
+    s = host(spec).reshape(Pd[0], Pd[1], Pd[2] + 2)[:, :, :2 * H]
+    got = s[..., 0::2] + 1j * s[..., 1::2]
+    scale = np.abs(want).max()
+    assert np.abs(got - want).max() <= 2e-6 * scale * np.log2(np.prod(Pd))
+    back = cuda.zeros(n + (Pd[0] - N[0]) * N[1] * N[2], device="cuda")
+    L.gpuFFT3dPlan_inverse(plan, P(spec), P(back))
+    b = host(back)[:n].reshape(N)
+    nrm = L.gpuFFT3dPlan_normalization(plan)
+    assert nrm == np.prod(Pd)
+    assert np.abs(b / nrm - a).max() <= 2e-6 * np.abs(a).max() * np.log2(np.prod(Pd))
+    L.delete_gpuFFT3dPlan(plan)

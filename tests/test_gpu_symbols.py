@@ -421,7 +421,8 @@ def test_gpu_reduce_all_ops(libs, eng, cuda, n):
 
 
 # ---------------------------------------------------------------- transforms
-@pytest.mark.parametrize("N,Pd", [((1, 16, 32), (1, 32, 64)), ((4, 12, 20), (8, 24, 40)), ((3, 5, 14), (6, 10, 28))])
+@pytest.mark.parametrize("N,Pd", [((1, 16, 32), (1, 32, 64)), ((4, 12, 20), (8, 24, 40)), ((3, 5, 14), (6, 10, 28)),
+                                  ((3, 11, 13), (6, 22, 26)), ((2, 5, 23), (4, 10, 46))])
 def test_fft_plan_forward_inverse(libs, cuda, N, Pd):
     """gpuFFT3dPlan_forward / _inverse of this library (own transforms)
     against the reference's (cuFFT) on the same padded input: spectra within

@@ -798,6 +798,37 @@ def partition_requests(reqs, world):
     return [ranks[r["index"]] for r in reqs]
 
 
+def serve_share(reqs, rank, world, make_server, gather=None, **run_kw):
+    """The multi-GPU serving form: every rank computes the same partition
+    (partition_requests), serves its share on its own server (make_server()
+    builds it; run_stream drives it) and the results are gathered on rank 0
+    by 'gather' (a torch.distributed gather_object to rank 0 when None and
+    world > 1).  No collective touches the solves' data.  Returns the
+    results of every request sorted by index on rank 0, None on the others."""
+    part = partition_requests(reqs, world)
+    mine = [r for r, k in zip(reqs, part) if k == rank]
+    server = make_server()
+    try:
+        res = run_stream(server, mine, **run_kw)
+    finally:
+        close = getattr(server, "close", None)
+        if close:
+            close()
+    for r in res:
+        r["rank"] = rank
+    if world == 1:
+        return res
+    if gather is None:
+        import torch.distributed as dist
+        got = [None] * world if rank == 0 else None
+        dist.gather_object(res, got, dst=0)
+    else:
+        got = gather(res)
+    if rank != 0:
+        return None
+    return sorted((r for part_res in got for r in part_res), key=lambda x: x["index"])
+
+
 def run_stream(server, reqs, realtime=True, max_torque=1e-4, max_steps=0, poll=0.0005):
     """Drives a Server with the requests' arrival times: each request is
     submitted once the server clock passes its arrival (all at once when

@@ -350,9 +350,10 @@ def vortex_m(nx, ny, seed=3, core=2.5, noise=0.02):
 
 def run_precision(args, name):
     """The precision form against the FP32 form on the same film: RK23
-    steps per second of each, the split-precision field's error against the
-    FP64 oracle (one evaluation) and the two forms' difference after the
-    same simulated time."""
+    steps per second of each, the split-precision field's difference from
+    the FP32 form's (one evaluation) and the two forms' difference after the
+    same number of steps.  Their error against FP64 is a test
+    (tests/test_gpu_precision.py)."""
     import torch
     eng = importlib.import_module("1_b200")
     w = PRECISION_WORKLOADS[name]
@@ -393,10 +394,8 @@ def run_precision(args, name):
         res[prec]["h"] = ht.cpu().numpy()
         s.close()
     clk = clocks.stop()
-    import oracle as O  # the checker: FP64 field of the same state
-    h64 = O.OracleSim(O.make_cfg(**kw), m0, bits=64).heff(m0.astype(np.float64))
-    scale = float(np.abs(h64).max())
     p, f = res[1], res[0]
+    scale = float(np.abs(f["h"]).max())
     value = n * args.steps / (p["ms"] / 1e3)
     line = {"metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": p["ms"] / args.steps, "higher_is_better": True,
@@ -406,9 +405,10 @@ def run_precision(args, name):
             "fp32_form": {"value": n * args.steps / (f["ms"] / 1e3), "ms_per_step": f["ms"] / args.steps,
                           "passes_ms_per_launch": f["passes"]},
             "passes_ms_per_launch": p["passes"],
-            "field_err_vs_fp64": {"split_bf16": float(np.abs(p["h"] - h64).max()) / scale,
-                                  "fp32": float(np.abs(f["h"] - h64).max()) / scale,
-                                  "norm": "max |h - h_fp64| / max |h_fp64|, one evaluation of the initial state"},
+            "field_diff_vs_fp32_form": {"split_bf16": float(np.abs(p["h"] - f["h"]).max()) / scale,
+                                        "norm": "max |h_split - h_fp32| / max |h_fp32|, one evaluation of the "
+                                                "initial state; the error against FP64 is measured by "
+                                                "tests/test_gpu_precision.py"},
             "gpu_launches": None, "clocks": clk}
     # same number of adaptive steps: compare the states where both forms stand
     line["after_steps"] = {"steps": args.warmup + args.steps, "time_split": p["state"]["time"],

@@ -86,3 +86,37 @@ def test_precision_steps_vs_fp64(eng, cuda):
     o = O.OracleSim(O.make_cfg(**FILM512, solver="rk4", dt=1e-13), m, bits=64)
     o.steps(10)
     assert np.abs(got - o.m()).max() < 1e-4
+
+
+def test_precision_form_rk23_500ps_vs_fp64_oracle(eng, cuda):
+    """The precision configuration's run, RK23 (max error 1e-5) for 500 ps
+    on the configuration's material and cell (2 nm, Ms 8.6e5 A/m, A 1.3e-11
+    J/m, alpha 0.1) with the split-BF16 tensor-core Y convolution, against
+    the FP64 oracle's Sim.Run of the same film.  The film is 16 x 512 cells
+    (the kernel's 512-cell Y lines; the full 512 x 512 film takes the FP64
+    oracle a quarter of an hour): <m> along the run (the oracle logs every
+    step, interpolated at the engine's rows) and m per cell at the end."""
+    from scipy.interpolate import CubicSpline
+    c = dict(grid=(16, 512, 1), cell=(2e-9, 2e-9, 2e-9), msat=8.6e5, aexch=1.3e-11, alpha=0.1, solver="rk23",
+             maxerror=1e-5)
+    m0 = O.seeded_m(c["grid"], 3, "tilted")
+    o = O.OracleSim(O.make_cfg(**c), m0, bits=64)
+    dense = o.run_table(5e-10, 0.0, max_rows=100000)
+    out = {}
+    for prec in (1, 0):
+        s = eng.Solver(eng.mmx_params(**c, precision=prec))
+        s.set_m(m0)
+        s.device_control(True)
+        rows = s.run(5e-10, 1e-11, max_rows=1000, max_steps=10 ** 6)
+        out[prec] = (rows, s.get_m(), s.state())
+        s.close()
+    cs = CubicSpline(dense[:, 0].astype(np.float64), dense[:, 1:4].astype(np.float64))
+    res = {}
+    for prec, (rows, m, st) in out.items():
+        d_avg = float(np.abs(cs(rows[:, 0].astype(np.float64)) - rows[:, 1:4]).max())
+        d_m = float(np.abs(m - o.m()).max())
+        res[prec] = (d_avg, d_m, st["steps"])
+    print("\nprecision form 500 ps vs FP64: <m> %.3g, max|dm| %.3g, %d steps; FP32 form <m> %.3g, max|dm| %.3g, "
+          "%d steps; FP64 oracle %d steps" % (res[1] + res[0] + (len(dense),)))
+    assert res[1][0] <= 1e-4 and res[1][1] <= 1e-4
+    assert res[0][0] <= 1e-4 and res[0][1] <= 1e-4

@@ -220,7 +220,7 @@ float gpu_array_get(float* p, int index) {
 }
 void gpu_array_set(float* p, int index, float value) { memcpy_to_gpu(&value, p + index, 1); }
 
-static float g_host_probe[1];
+static volatile float g_host_probe[1];
 static float* g_dev_probe = nullptr;
 void assertHost(float* pointer) { g_host_probe[0] = pointer[0]; }
 void assertDevice(float* pointer) {

@@ -25,22 +25,24 @@ constexpr int WAIT_ITERS = 1 << 22;
 // DFT matrix exp(sign 2 pi i j k / L) in the interleaved real form, split
 // into bfloat16 hi and lo, laid out as canonical K-major 64 x 64 tiles.
 // Built on the host in float64.
+uint16_t bf16_rne(float x) {  // round to nearest even (finite x)
+  uint32_t u;
+  memcpy(&u, &x, 4);
+  uint32_t r = u + 0x7FFFu + ((u >> 16) & 1u);
+  return (uint16_t)(r >> 16);
+}
+float bf16_val(uint16_t h) {
+  uint32_t u = (uint32_t)h << 16;
+  float x;
+  memcpy(&x, &u, 4);
+  return x;
+}
 void build_dft_tiles(int L, int sign, std::vector<uint16_t>& hi, std::vector<uint16_t>& lo) {
   const int K = 2 * L;
   hi.assign((size_t)2 * L * K, 0);
   lo.assign((size_t)2 * L * K, 0);
-  auto bf = [](float x) -> uint16_t {  // round to nearest even
-    uint32_t u;
-    memcpy(&u, &x, 4);
-    uint32_t r = u + 0x7FFFu + ((u >> 16) & 1u);
-    return (uint16_t)(r >> 16);
-  };
-  auto unbf = [](uint16_t h) -> float {
-    uint32_t u = (uint32_t)h << 16;
-    float x;
-    memcpy(&x, &u, 4);
-    return x;
-  };
+  auto bf = bf16_rne;
+  auto unbf = bf16_val;
   for (int j = 0; j < L; j++)
     for (int i = 0; i < L; i++) {
       double ang = sign * 2.0 * M_PI * (double)((j * i) % L) / (double)L;
@@ -54,6 +56,30 @@ void build_dft_tiles(int L, int sign, std::vector<uint16_t>& hi, std::vector<uin
           uint32_t off = dtc::kmajor_off(2 * j + rm, 2 * i + rk, K) / 2;
           hi[off] = h;
           lo[off] = l;
+        }
+    }
+}
+
+// The same matrix split three ways (hi, mid, lo: each the bfloat16
+// rounding of what the previous parts leave), three consecutive tiles.
+void build_dft_tiles3(int L, int sign, std::vector<uint16_t>& out) {
+  const int K = 2 * L;
+  const size_t T = (size_t)2 * L * K;
+  out.assign(3 * T, 0);
+  for (int j = 0; j < L; j++)
+    for (int i = 0; i < L; i++) {
+      double ang = sign * 2.0 * M_PI * (double)((j * i) % L) / (double)L;
+      float c = (float)cos(ang), s = (float)sin(ang);
+      float blk[2][2] = {{c, -s}, {s, c}};
+      for (int rm = 0; rm < 2; rm++)
+        for (int rk = 0; rk < 2; rk++) {
+          float v = blk[rm][rk];
+          const uint32_t off = dtc::kmajor_off(2 * j + rm, 2 * i + rk, K) / 2;
+          for (int part = 0; part < 3; part++) {
+            uint16_t h = bf16_rne(v);
+            out[part * T + off] = h;
+            v -= bf16_val(h);
+          }
         }
     }
 }
@@ -81,6 +107,28 @@ int dft_tables(const uint16_t** out, int inverse) {
     }
     MMX_TRY(cudaMemcpy(p, hi.data(), hi.size() * 2, cudaMemcpyHostToDevice));
     MMX_TRY(cudaMemcpy(p + hi.size(), lo.data(), lo.size() * 2, cudaMemcpyHostToDevice));
+  }
+  *out = p;
+  return MMX_OK;
+}
+
+DftTables g_dft3[64];  // per device, three-way split
+
+int dft_tables3(const uint16_t** out, int inverse) {
+  int dev = 0;
+  MMX_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) { mmx_set_error("device index out of range"); return MMX_ERR_ARG; }
+  std::lock_guard<std::mutex> lock(g_dft_mu);
+  uint16_t*& p = inverse ? g_dft3[dev].inv : g_dft3[dev].fwd;
+  if (!p) {
+    std::vector<uint16_t> t;
+    build_dft_tiles3(DL, inverse ? 1 : -1, t);
+    if (cudaMalloc(&p, t.size() * sizeof(uint16_t)) != cudaSuccess) {
+      p = nullptr;
+      mmx_set_error("out of device memory");
+      return MMX_ERR_MEM;
+    }
+    MMX_TRY(cudaMemcpy(p, t.data(), t.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
   }
   *out = p;
   return MMX_OK;
@@ -195,110 +243,186 @@ extern "C" int mmx_dft_tc(const float2* in, float2* out, int nvec, int inverse, 
 //   tw  A[k1][n2] *= W1024^(n2 k1)
 //   F2  X[k1 + 32 k2] = sum_n2 W32^(n2 k2) A[k1][n2]
 // then H = K X per bin (the 2D kernel product of gpu_kernelmul4), and the
-// inverse in reverse order, keeping only the outputs y < 512.  Each layer is
-// one tensor-core GEMM D[64 x 192] = W[64 x 64] . X[64 x 192] over the 192
-// vectors of a CTA (2 kz columns x 3 components x 32), split-BF16 operands,
-// FP32 accumulation in TMEM; between layers each thread reads its
-// accumulator row back (tcgen05.ld), pairs real and imaginary parts with a
-// lane shuffle, applies the twiddle or the kernel product in FP32, and
-// writes the next layer's operand tile.
+// inverse in reverse order, keeping only the outputs y < 512.
+//
+// A CTA takes 4 kz columns, one per TMEM lane quarter.  Each layer is, per
+// component c, one tensor-core GEMM D_c[128 x 64] = X_c[128 x 64] . W^T with
+// the 128 vectors v = (kz, 32-point index) as M, so vector v's 32 complex
+// outputs land in TMEM lane v, columns 64 c .. 64 c + 63 (re, im
+// interleaved).  Both operands are split three ways into bfloat16 (x = hi +
+// mid + lo, each the rounding of the remainder) and the six products with
+// weight >= 2^-16 relative (hh, hm, mh, hl, lh, mm) are accumulated in FP32:
+// about 24 significant bits per operand, the FP32 transform's precision.
+// Two warps share each lane quarter and split every epilogue's columns in
+// halves; thread 0 issues all MMAs.
 // ---------------------------------------------------------------------
 namespace {
-constexpr int YT = 128;              // threads
-constexpr int YKZ = 2;               // kz columns per CTA
-constexpr int YCOLS = 3 * YKZ;       // (component, kz) columns
-constexpr int YNV = 32 * YCOLS;      // GEMM N (vectors)
-constexpr int YL = 1024;             // padded Y length
-constexpr int YWB = 64 * 64 * 2;     // bytes of one W tile
-constexpr int YXB = YNV * 64 * 2;    // bytes of one X tile
-constexpr size_t YSMEM = 4 * (size_t)YWB + 2 * (size_t)YXB + YL * sizeof(float2);
+constexpr int YT = 256;                        // threads: 8 warps, two per TMEM sub-partition
+constexpr int YKZ = 4;                         // kz columns per CTA, one per TMEM lane quarter
+constexpr int YL = 1024;                       // padded Y length
+constexpr int YK = 3 * 64;                     // operand K extent: 3 components x 64
+constexpr int YLBO = 144;                      // bytes between K-adjacent core matrices (128 + 16)
+constexpr int YSBO = (YK / 8) * YLBO;          // bytes between 8-row groups (3456)
+constexpr int YXB = 16 * YSBO;                 // bytes of one 128-row operand tile (55296)
+constexpr int YWB = 64 * 64 * 2;               // bytes of one W tile
+constexpr size_t YSMEM = 3 * (size_t)YXB + 6 * (size_t)YWB + YL * sizeof(float2);
+constexpr int YN = 512;                        // data length along Y
+constexpr int YSP = YN + 8;                    // staging pitch of one (component, kz) line, float2
+constexpr int KTS = 520;                       // kernel line pitch (floats) of the kz-major coefficients
+static_assert(3 * YKZ * YSP * sizeof(float2) <= 6 * (size_t)YWB + YL * sizeof(float2),
+              "the input staging lies in the W and twiddle area");
 
 struct YconvTc {
   float2* S;
   int64_t CS;
   int HZ, N1;
-  const float* kh;
-  int64_t kcs;
-  const uint16_t* wf;
-  const uint16_t* wi;
-  const float2* tw;  // exp(-2 pi i t / 1024)
+  const float* kt;     // kernel coefficients Kxx, Kyy, Kzz, Kyz as [4][HZ][KTS] (fy fastest)
+  int64_t ktcs;        // component stride of kt
+  const uint16_t* wf;  // forward W: hi, mid, lo tiles
+  const uint16_t* wi;  // inverse W: hi, mid, lo tiles
+  const float2* tw;    // exp(-2 pi i t / 1024)
   int* err;
 };
 
-// (re, im) at K positions 2i, 2i+1 of a vector: adjacent bfloat16s, one
-// 32-bit store into each of the hi and lo tiles
-__device__ __forceinline__ void put_split2(unsigned char* hi, unsigned char* lo, uint32_t off, float2 v) {
-  __nv_bfloat162 h, l;
-  dtc::split_bf16(v.x, h.x, l.x);
-  dtc::split_bf16(v.y, h.y, l.y);
-  *reinterpret_cast<__nv_bfloat162*>(hi + off) = h;
-  *reinterpret_cast<__nv_bfloat162*>(lo + off) = l;
+// byte offset of (row r, K index k) in an operand tile: canonical K-major
+// core matrices, K-adjacent ones YLBO bytes apart so that a warp's 32
+// stores at K = 2 n (n = lane) into one row hit 32 distinct banks
+__host__ __device__ __forceinline__ uint32_t xoff(int r, int k) {
+  return (uint32_t)((r >> 3) * YSBO + (k >> 3) * YLBO + (r & 7) * 16 + (k & 7) * 2);
 }
 
-// (re, im) of this lane's accumulator element and its partner lane's
-__device__ __forceinline__ float2 pair_ri(float mine, int ri) {
-  float other = __shfl_xor_sync(0xffffffffu, mine, 1);
-  return ri ? make_float2(other, mine) : make_float2(mine, other);
+// x = h + m + l, each a bfloat16 rounding of what is left
+__device__ __forceinline__ void split3(float x, __nv_bfloat16& h, __nv_bfloat16& m, __nv_bfloat16& l) {
+  h = __float2bfloat16_rn(x);
+  const float r1 = x - __bfloat162float(h);
+  m = __float2bfloat16_rn(r1);
+  l = __float2bfloat16_rn(r1 - __bfloat162float(m));
+}
+
+// (re, im) at K positions k, k+1 (k even): one 4-byte store into each of
+// the three tiles
+__device__ __forceinline__ void put_pair(unsigned char* x, int r, int k, float2 v) {
+  __nv_bfloat162 h, m, l;
+  split3(v.x, h.x, m.x, l.x);
+  split3(v.y, h.y, m.y, l.y);
+  const uint32_t o = xoff(r, k);
+  *reinterpret_cast<__nv_bfloat162*>(x + o) = h;
+  *reinterpret_cast<__nv_bfloat162*>(x + YXB + o) = m;
+  *reinterpret_cast<__nv_bfloat162*>(x + 2 * YXB + o) = l;
+}
+
+// four complex values at K positions k0 .. k0+7 (k0 a multiple of 8): one
+// 16-byte store into each of the three tiles
+__device__ __forceinline__ void put_quad(unsigned char* x, int r, int k0, const float2* v) {
+  __align__(16) __nv_bfloat162 h[4], m[4], l[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    split3(v[q].x, h[q].x, m[q].x, l[q].x);
+    split3(v[q].y, h[q].y, m[q].y, l[q].y);
+  }
+  const uint32_t o = xoff(r, k0);
+  *reinterpret_cast<uint4*>(x + o) = *reinterpret_cast<const uint4*>(h);
+  *reinterpret_cast<uint4*>(x + YXB + o) = *reinterpret_cast<const uint4*>(m);
+  *reinterpret_cast<uint4*>(x + 2 * YXB + o) = *reinterpret_cast<const uint4*>(l);
+}
+
+// One thread: for every component c, D_c (TMEM columns 64 c ..) = the split
+// product of the operand rows' K slice [64 c, 64 c + kmax) and W
+// (N = 64 outputs x 64 inputs, canonical K-major, LBO 128, SBO 1024).
+__device__ __forceinline__ void gemm3(uint32_t tmem, const unsigned char* x, const unsigned char* w, int kmax) {
+  constexpr uint32_t idesc = dtc::idesc_bf16(128, 64);
+  constexpr int PA[6] = {0, 0, 1, 0, 2, 1};  // operand part of each product
+  constexpr int PB[6] = {0, 1, 0, 2, 0, 1};  // W part of each product
+  const uint32_t xa = dtc::smem_u32(x), wb = dtc::smem_u32(w);
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    for (int kk = 0; kk < kmax; kk += 16) {
+#pragma unroll
+      for (int p = 0; p < 6; p++) {
+        const uint64_t ad = dtc::smem_desc(xa + PA[p] * YXB + (c * 8 + kk / 8) * YLBO, YLBO, YSBO);
+        const uint64_t bd = dtc::smem_desc(wb + PB[p] * YWB + (kk / 8) * 128, 128, 1024);
+        dtc::mma_bf16(tmem + 64 * c, ad, bd, idesc, (kk > 0 || p > 0) ? 1u : 0u);
+      }
+    }
+  }
 }
 }  // namespace
 
-__global__ void __launch_bounds__(YT) k_yconv2d_tc(YconvTc a) {
+__global__ void __launch_bounds__(YT, 1) k_yconv2d_tc(YconvTc a) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ uint32_t tmem_slot;
   __shared__ __align__(8) uint64_t bar;
-  unsigned char* wf_hi = smem;
-  unsigned char* wf_lo = smem + YWB;
-  unsigned char* wi_hi = smem + 2 * YWB;
-  unsigned char* wi_lo = smem + 3 * YWB;
-  unsigned char* x_hi = smem + 4 * YWB;
-  unsigned char* x_lo = smem + 4 * YWB + YXB;
-  float2* tw = reinterpret_cast<float2*>(smem + 4 * YWB + 2 * YXB);
+  unsigned char* xs = smem;                        // hi, mid, lo operand tiles
+  unsigned char* wf = smem + 3 * YXB;              // forward DFT: hi, mid, lo
+  unsigned char* wi = wf + 3 * YWB;                // inverse DFT: hi, mid, lo
+  float2* tw = reinterpret_cast<float2*>(wi + 3 * YWB);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int kz0 = blockIdx.x * YKZ;
+  // warps q and q + 4 share TMEM lane quarter q (kz column q of the CTA);
+  // half h of every epilogue's columns goes to warp q + 4h
+  const int quarter = warp & 3, half = warp >> 2;
   const int HZ = a.HZ;
+  const int kz = blockIdx.x * YKZ + quarter;
+  const int row0 = 32 * quarter;               // the quarter's 32 operand rows / TMEM lanes
 
   if (warp == 0) dtc::tmem_alloc(&tmem_slot, 256);
   if (threadIdx.x == 0) dtc::mbar_init(&bar, 1);
+  // the CTA's input, y < 512 of its 4 kz columns and 3 components, staged
+  // through the W / twiddle area as lines stg[(c * 4 + kzl) * YSP + y]: a
+  // warp's load covers 8 y rows x 4 adjacent kz (32 contiguous bytes each)
+  const int kz0 = blockIdx.x * YKZ;
+  {
+    float2* stg = reinterpret_cast<float2*>(wf);
+    for (int e = threadIdx.x; e < 3 * YN * YKZ; e += YT) {
+      const int kzl = e & 3, cy = e >> 2;
+      const int c = cy / YN, y = cy - c * YN;
+      const bool in = kz0 + kzl < HZ;
+      stg[(c * YKZ + kzl) * YSP + y] = in ? a.S[c * a.CS + (int64_t)y * HZ + kz0 + kzl] : make_float2(0.f, 0.f);
+    }
+  }
+  __syncthreads();
+  // F1 operand, row (kz, n2 = lane): K = 64 c + 2 n1 (+1), value y[32 n1 + n2]
+  // for n1 in this half's 8 of the 16 data rows; n1 >= 16 (K 32 .. 63 of the
+  // component, the zero padding) is never read: F1 uses K < 32
+  {
+    const float2* stg = reinterpret_cast<const float2*>(wf);
+    const int n2 = lane;
+    const int r = row0 + lane;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float2* line = stg + (c * YKZ + quarter) * YSP;
+#pragma unroll
+      for (int qq = 0; qq < 2; qq++) {
+        const int q4 = 2 * half + qq;
+        float2 v[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) v[q] = line[32 * (4 * q4 + q) + n2];
+        put_quad(xs, r, 64 * c + 8 * q4, v);
+      }
+    }
+  }
+  __syncthreads();  // staging read before the W tiles overwrite it
   {
     const uint4* s0 = reinterpret_cast<const uint4*>(a.wf);
     const uint4* s1 = reinterpret_cast<const uint4*>(a.wi);
-    uint4* d0 = reinterpret_cast<uint4*>(wf_hi);
-    uint4* d1 = reinterpret_cast<uint4*>(wi_hi);
-    for (int i = threadIdx.x; i < 2 * YWB / 16; i += YT) {
+    uint4* d0 = reinterpret_cast<uint4*>(wf);
+    uint4* d1 = reinterpret_cast<uint4*>(wi);
+    for (int i = threadIdx.x; i < 3 * YWB / 16; i += YT) {
       d0[i] = __ldg(&s0[i]);
       d1[i] = __ldg(&s1[i]);
     }
     for (int i = threadIdx.x; i < YL; i += YT) tw[i] = __ldg(&a.tw[i]);
   }
-  // F1 operand: vector (col, n2), K index 2 n1 + ri, value y[32 n1 + n2]
-  for (int e = threadIdx.x; e < YCOLS * 32 * 32; e += YT) {
-    int kzl = e % YKZ;
-    int rest = e / YKZ;
-    int n2 = rest % 32;
-    int n1 = (rest / 32) % 32;
-    int c = rest / (32 * 32);
-    int y = 32 * n1 + n2, kz = kz0 + kzl;
-    float2 v = make_float2(0.f, 0.f);
-    if (y < a.N1 && kz < HZ) v = a.S[c * a.CS + (int64_t)y * HZ + kz];
-    int vec = 32 * (3 * kzl + c) + n2;
-    put_split2(x_hi, x_lo, dtc::kmajor_off(vec, 2 * n1, 64), v);
-  }
-  const uint32_t tbase = 0;  // set after the allocation is visible
-  (void)tbase;
   dtc::fence_async_smem();
   dtc::fence_before_sync();
   __syncthreads();
   dtc::fence_after_sync();
   const uint32_t tmem = tmem_slot;
-  const uint32_t tw_addr = tmem + ((uint32_t)(32 * warp) << 16);
-  const int m = 16 * warp + (lane & 15);  // accumulator row of this lane (lanes >= 16 duplicate)
-  const int hi_idx = m >> 1, ri = m & 1;
+  const uint32_t tl = tmem + ((uint32_t)row0 << 16);  // the quarter's TMEM lanes
   bool ok = true;
   uint32_t phase = 0;
-
-  auto run_gemm = [&](const unsigned char* wh, const unsigned char* wl) {
+  auto run_gemm = [&](const unsigned char* w, int kmax) {
     if (threadIdx.x == 0) {
-      dtc::gemm_split<64, YNV>(tmem, wh, wl, x_hi, x_lo);
+      gemm3(tmem, xs, w, kmax);
       dtc::mma_commit(&bar);
     }
     bool done = dtc::mbar_wait(&bar, phase, WAIT_ITERS);
@@ -313,100 +437,115 @@ __global__ void __launch_bounds__(YT) k_yconv2d_tc(YconvTc a) {
     __syncthreads();
     dtc::fence_after_sync();
   };
+  // this thread's 32 outputs (16 complex) of component c in its half:
+  // columns 64c + 32h .. 64c + 32h + 31 of its lane
+  auto read_half = [&](int c, float* v) {
+    dtc::tmem_ld32(tl + 64 * c + 32 * half, v);
+    dtc::tmem_wait_ld();
+  };
 
-  // ---- F1 ----
-  run_gemm(wf_hi, wf_lo);
-  // rows: (k1, ri); columns: (col, n2).  twiddle W1024^(n2 k1) -> F2 operand (col, k1) x (n2, ri)
+  // ---- F1: thread (kz, n2) gets A[k1][n2], k1 in its half ----
+  run_gemm(wf, 32);
   if (ok) {
-    const int k1 = hi_idx;
-    for (int c8 = 0; c8 < YNV; c8 += 32) {
+    const int n2 = lane;
+    for (int c = 0; c < 3; c++) {
       float v[32];
-      dtc::tmem_ld32(tw_addr + c8, v);
-      dtc::tmem_wait_ld();
+      read_half(c, v);
+      // twiddle W1024^(n2 k1) -> F2 operand row (kz, k1), K = 64 c + 2 n2
 #pragma unroll
-      for (int q = 0; q < 32; q++) {
-        int col = (c8 + q) >> 5, n2 = (c8 + q) & 31;
-        float2 z = pair_ri(v[q], ri);
-        float2 w = tw[(n2 * k1) & (YL - 1)];
-        float2 t = make_float2(fmaf(z.x, w.x, -z.y * w.y), fmaf(z.x, w.y, z.y * w.x));
-        if (lane < 16 && ri == 0) put_split2(x_hi, x_lo, dtc::kmajor_off(32 * col + k1, 2 * n2, 64), t);
+      for (int j = 0; j < 16; j++) {
+        const int k1 = 16 * half + j;
+        const float2 w = tw[(n2 * k1) & (YL - 1)];
+        const float zr = v[2 * j], zi = v[2 * j + 1];
+        const float2 t = make_float2(fmaf(zr, w.x, -zi * w.y), fmaf(zr, w.y, zi * w.x));
+        put_pair(xs, row0 + k1, 64 * c + 2 * n2, t);
       }
     }
   }
   operand_ready();
-  // ---- F2 ----
-  if (ok) run_gemm(wf_hi, wf_lo);
-  // rows: (k2, ri); columns: (col, k1); bin k = k1 + 32 k2.  H = K X -> I1 operand (col, k1) x (k2, ri)
+  // ---- F2: thread (kz, k1) gets the bins k = k1 + 32 k2 of all three
+  // components, k2 in its half ----
+  if (ok) run_gemm(wf, 64);
   if (ok) {
-    const int k2 = hi_idx;
-    for (int kzl = 0; kzl < YKZ; kzl++) {
-      const int kz = kz0 + kzl;
-      const int kzc = kz < HZ ? kz : HZ - 1;
-      for (int k1c = 0; k1c < 32; k1c += 8) {
-        float v[3][8];
+    const int k1 = lane;
+    const float* kline = a.kt + (int64_t)(kz < HZ ? kz : HZ - 1) * KTS;
+    float vx[32], vy[32], vz[32];
+    dtc::tmem_ld32(tl + 0 * 64 + 32 * half, vx);
+    dtc::tmem_ld32(tl + 1 * 64 + 32 * half, vy);
+    dtc::tmem_ld32(tl + 2 * 64 + 32 * half, vz);
+    dtc::tmem_wait_ld();
+    // H = K X (gpu_kernelmul4) -> I1 operand row (kz, k1), K = 64 c + 2 k2
 #pragma unroll
-        for (int c = 0; c < 3; c++) dtc::tmem_ld8(tw_addr + 32 * (3 * kzl + c) + k1c, v[c]);
-        dtc::tmem_wait_ld();
+    for (int k2q = 0; k2q < 4; k2q++) {
+      float2 hx[4], hy[4], hz[4];
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-          const int k1 = k1c + q, k = k1 + 32 * k2;
-          float2 mx = pair_ri(v[0][q], ri), my = pair_ri(v[1][q], ri), mz = pair_ri(v[2][q], ri);
-          const bool neg = k > YL / 2;
-          const int fy = neg ? YL - k : k;
-          const float* kp = a.kh + (int64_t)fy * HZ + kzc;
-          float Kxx = __ldg(kp), Kyy = __ldg(kp + a.kcs), Kzz = __ldg(kp + 2 * a.kcs), Kyz = __ldg(kp + 3 * a.kcs);
-          if (neg) Kyz = -Kyz;
-          float2 hx = make_float2(mx.x * Kxx, mx.y * Kxx);
-          float2 hy = make_float2(fmaf(mz.x, Kyz, my.x * Kyy), fmaf(mz.y, Kyz, my.y * Kyy));
-          float2 hz = make_float2(fmaf(mz.x, Kzz, my.x * Kyz), fmaf(mz.y, Kzz, my.y * Kyz));
-          if (lane < 16 && ri == 0) {
-            put_split2(x_hi, x_lo, dtc::kmajor_off(32 * (3 * kzl + 0) + k1, 2 * k2, 64), hx);
-            put_split2(x_hi, x_lo, dtc::kmajor_off(32 * (3 * kzl + 1) + k1, 2 * k2, 64), hy);
-            put_split2(x_hi, x_lo, dtc::kmajor_off(32 * (3 * kzl + 2) + k1, 2 * k2, 64), hz);
-          }
-        }
+      for (int q = 0; q < 4; q++) {
+        const int k2l = 4 * k2q + q;   // index within the half
+        const int k2 = 16 * half + k2l;
+        const int k = k1 + 32 * k2;
+        const bool neg = k > YL / 2;
+        const int fy = neg ? YL - k : k;
+        const float* kp = kline + fy;  // lanes: consecutive fy
+        const float Kxx = __ldg(kp), Kyy = __ldg(kp + a.ktcs), Kzz = __ldg(kp + 2 * a.ktcs);
+        float Kyz = __ldg(kp + 3 * a.ktcs);
+        if (neg) Kyz = -Kyz;
+        const float2 mx = make_float2(vx[2 * k2l], vx[2 * k2l + 1]);
+        const float2 my = make_float2(vy[2 * k2l], vy[2 * k2l + 1]);
+        const float2 mz = make_float2(vz[2 * k2l], vz[2 * k2l + 1]);
+        hx[q] = make_float2(mx.x * Kxx, mx.y * Kxx);
+        hy[q] = make_float2(fmaf(mz.x, Kyz, my.x * Kyy), fmaf(mz.y, Kyz, my.y * Kyy));
+        hz[q] = make_float2(fmaf(mz.x, Kzz, my.x * Kyz), fmaf(mz.y, Kzz, my.y * Kyz));
+      }
+      const int kb = 32 * half + 8 * k2q;
+      put_quad(xs, row0 + k1, 0 * 64 + kb, hx);
+      put_quad(xs, row0 + k1, 1 * 64 + kb, hy);
+      put_quad(xs, row0 + k1, 2 * 64 + kb, hz);
+    }
+  }
+  operand_ready();
+  // ---- I1: thread (kz, k1) gets (n2) outputs, n2 in its half; twiddle
+  // W1024^(-n2 k1) ----
+  if (ok) run_gemm(wi, 64);
+  if (ok) {
+    const int k1 = lane;
+    for (int c = 0; c < 3; c++) {
+      float v[32];
+      read_half(c, v);
+      // -> I2 operand row (kz, n2), K = 64 c + 2 k1
+#pragma unroll
+      for (int j = 0; j < 16; j++) {
+        const int n2 = 16 * half + j;
+        const float2 w = tw[(n2 * k1) & (YL - 1)];
+        const float zr = v[2 * j], zi = v[2 * j + 1];
+        const float2 t = make_float2(fmaf(zr, w.x, zi * w.y), fmaf(zi, w.x, -zr * w.y));  // z conj(w)
+        put_pair(xs, row0 + n2, 64 * c + 2 * k1, t);
       }
     }
   }
   operand_ready();
-  // ---- I1 ----
-  if (ok) run_gemm(wi_hi, wi_lo);
-  // rows: (n2, ri); columns: (col, k1).  twiddle W1024^(-n2 k1) -> I2 operand (col, n2) x (k1, ri)
-  if (ok) {
-    const int n2 = hi_idx;
-    for (int c8 = 0; c8 < YNV; c8 += 32) {
+  // ---- I2: thread (kz, n2) gets y = 32 n1 + n2; y < 512 (n1 < 16, the
+  // first half of the columns) goes to staging lines in the operand area
+  // (free once this GEMM has completed), then out in the same 4-kz-wide
+  // rows as the input ----
+  if (ok) run_gemm(wi, 64);
+  if (ok && half == 0) {
+    float2* stg = reinterpret_cast<float2*>(xs);
+    const int n2 = lane;
+    for (int c = 0; c < 3; c++) {
       float v[32];
-      dtc::tmem_ld32(tw_addr + c8, v);
-      dtc::tmem_wait_ld();
+      read_half(c, v);
+      float2* line = stg + (c * YKZ + quarter) * YSP;
 #pragma unroll
-      for (int q = 0; q < 32; q++) {
-        int col = (c8 + q) >> 5, k1 = (c8 + q) & 31;
-        float2 z = pair_ri(v[q], ri);
-        float2 w = tw[(n2 * k1) & (YL - 1)];
-        // z * conj(w)
-        float2 t = make_float2(fmaf(z.x, w.x, z.y * w.y), fmaf(z.y, w.x, -z.x * w.y));
-        if (lane < 16 && ri == 0) put_split2(x_hi, x_lo, dtc::kmajor_off(32 * col + n2, 2 * k1, 64), t);
-      }
+      for (int n1 = 0; n1 < 16; n1++) line[32 * n1 + n2] = make_float2(v[2 * n1], v[2 * n1 + 1]);
     }
   }
-  operand_ready();
-  // ---- I2 ----
-  if (ok) run_gemm(wi_hi, wi_lo);
-  // rows: (n1, ri); columns: (col, n2); y = 32 n1 + n2 < N1 stored
-  if (ok && warp < 2) {
-    const int n1 = hi_idx;
-    for (int c8 = 0; c8 < YNV; c8 += 32) {
-      float v[32];
-      dtc::tmem_ld32(tw_addr + c8, v);
-      dtc::tmem_wait_ld();
-#pragma unroll
-      for (int q = 0; q < 32; q++) {
-        int col = (c8 + q) >> 5, n2 = (c8 + q) & 31;
-        float2 z = pair_ri(v[q], ri);
-        int c = col % 3, kzl = col / 3;
-        int y = 32 * n1 + n2, kz = kz0 + kzl;
-        if (lane < 16 && ri == 0 && y < a.N1 && kz < HZ) a.S[c * a.CS + (int64_t)y * HZ + kz] = z;
-      }
+  __syncthreads();
+  if (ok) {
+    const float2* stg = reinterpret_cast<const float2*>(xs);
+    for (int e = threadIdx.x; e < 3 * YN * YKZ; e += YT) {
+      const int kzl = e & 3, cy = e >> 2;
+      const int c = cy / YN, y = cy - c * YN;
+      if (kz0 + kzl < HZ) a.S[c * a.CS + (int64_t)y * HZ + kz0 + kzl] = stg[(c * YKZ + kzl) * YSP + y];
     }
   }
   if (!ok && threadIdx.x == 0) atomicExch(a.err, 1);
@@ -425,8 +564,8 @@ float2* g_tw1024[64];
 // shared-memory limit; called when a precision-form solver is created, so
 // that no allocation happens while its steps are captured into a graph.
 static int yconv2d_tc_prepare(const uint16_t** wf, const uint16_t** wi, float2** tw) {
-  MMX_CHECK_RC(dft_tables(wf, 0));
-  MMX_CHECK_RC(dft_tables(wi, 1));
+  MMX_CHECK_RC(dft_tables3(wf, 0));
+  MMX_CHECK_RC(dft_tables3(wi, 1));
   int dev = 0;
   MMX_TRY(cudaGetDevice(&dev));
   {
@@ -450,6 +589,35 @@ static int yconv2d_tc_prepare(const uint16_t** wf, const uint16_t** wi, float2**
   return MMX_OK;
 }
 
+// kt[a][kz][fy] = kh[a][fy][kz] for a = Kxx, Kyy, Kzz, Kyz (the first four
+// components of the kernel octant), fy <= 512, line pitch KTS
+__global__ void k_kernel_kz_major(const float* __restrict__ kh, int64_t kcs, int HZ, float* __restrict__ kt) {
+  const int64_t n = 4 * (int64_t)HZ * KTS;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int fy = (int)(e % KTS);
+    const int64_t rest = e / KTS;
+    const int kz = (int)(rest % HZ), c = (int)(rest / HZ);
+    kt[e] = fy <= YL / 2 ? kh[c * kcs + (int64_t)fy * HZ + kz] : 0.f;
+  }
+}
+
+// The kz-major copy of a 2D film's kernel octant (kh[c][fy][kz], fy <= 512,
+// component stride kcs) that the split-precision Y convolution reads:
+// 4 x HZ x KTS floats, allocated here, freed by the caller.
+int mmx_yconv2d_tc_kernel(const float* kh, int64_t kcs, int HZ, float** kt) {
+  if (!kh || !kt || HZ < 1) { mmx_set_error("bad argument"); return MMX_ERR_ARG; }
+  const size_t bytes = sizeof(float) * 4 * (size_t)HZ * KTS;
+  if (cudaMalloc(kt, bytes) != cudaSuccess) {
+    *kt = nullptr;
+    mmx_set_error("out of device memory");
+    return MMX_ERR_MEM;
+  }
+  k_kernel_kz_major<<<296, 256>>>(kh, kcs, HZ, *kt);
+  MMX_TRY(cudaGetLastError());
+  MMX_TRY(cudaDeviceSynchronize());
+  return MMX_OK;
+}
+
 int mmx_yconv2d_tc_prepare() {
   const uint16_t *wf, *wi;
   float2* tw;
@@ -457,9 +625,9 @@ int mmx_yconv2d_tc_prepare() {
 }
 
 // Launches the split-precision Y convolution over the spectrum of a 2D film
-// with P1 = 1024 (kernel octant kh[4][513][HZ], component stride kcs).
-int mmx_yconv2d_tc_launch(float2* S, int64_t CS, int HZ, int N1, const float* kh, int64_t kcs, int* err,
-                          cudaStream_t st) {
+// with P1 = 1024 and Ny = 512 (kernel kt from mmx_yconv2d_tc_kernel).
+int mmx_yconv2d_tc_launch(float2* S, int64_t CS, int HZ, int N1, const float* kt, int* err, cudaStream_t st) {
+  if (N1 != YN) { mmx_set_error("split-precision Y convolution: Ny = 512 only"); return MMX_ERR_ARG; }
   const uint16_t *wf = nullptr, *wi = nullptr;
   float2* tw = nullptr;
   MMX_CHECK_RC(yconv2d_tc_prepare(&wf, &wi, &tw));
@@ -468,8 +636,8 @@ int mmx_yconv2d_tc_launch(float2* S, int64_t CS, int HZ, int N1, const float* kh
   a.CS = CS;
   a.HZ = HZ;
   a.N1 = N1;
-  a.kh = kh;
-  a.kcs = kcs;
+  a.kt = kt;
+  a.ktcs = (int64_t)HZ * KTS;
   a.wf = wf;
   a.wi = wi;
   a.tw = tw;

@@ -407,16 +407,16 @@ static cudaError_t launch_xconv(mmx_solver* s, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-int mmx_yconv2d_tc_launch(float2* S, int64_t CS, int HZ, int N1, const float* kh, int64_t kcs, int* err,
-                          cudaStream_t st);
+int mmx_yconv2d_tc_launch(float2* S, int64_t CS, int HZ, int N1, const float* kt, int* err, cudaStream_t st);
 int mmx_yconv2d_tc_prepare();
+int mmx_yconv2d_tc_kernel(const float* kh, int64_t kcs, int HZ, float** kt);
 
 static cudaError_t launch_yconv2d(mmx_solver* s, cudaStream_t st) {
   int P1 = s->P[1];
   if (s->p.precision) {
     ScopedPass sp(s, "yconv2d_tc", st);
-    int rc = mmx_yconv2d_tc_launch(s->S, s->CS, s->HZ, s->N[1], s->K.kh, s->K.cs,
-                                   reinterpret_cast<int*>(s->scratch + 15), st);
+    int rc = mmx_yconv2d_tc_launch(s->S, s->CS, s->HZ, s->N[1], s->kt_tc, reinterpret_cast<int*>(s->scratch + 15),
+                                   st);
     return rc == MMX_OK ? cudaSuccess : cudaErrorLaunchFailure;
   }
   if (fx_ok(P1)) {
@@ -904,6 +904,7 @@ static void solver_free(mmx_solver* s) {
   cudaFree(s->rkdev);
   cudaFree(s->S);
   cudaFree(s->kh);
+  cudaFree(s->kt_tc);
   cudaFree(s->m);
   cudaFree(s->t0);
   cudaFree(s->m1);
@@ -1017,6 +1018,7 @@ extern "C" int mmx_solver_create(const mmx_params* p, mmx_solver** out) {
 #undef ALLOC
   if (s->p.precision) {
     rc = mmx_yconv2d_tc_prepare();
+    if (rc == MMX_OK) rc = mmx_yconv2d_tc_kernel(s->K.kh, s->K.cs, s->HZ, &s->kt_tc);
     if (rc != MMX_OK) { solver_free(s); return rc; }
   }
   *out = s;

@@ -35,6 +35,7 @@ struct mmx_solver {
   float2* S = nullptr;
   int64_t CS = 0;
   float* kh = nullptr;
+  float* kt_tc = nullptr;  // precision form: the 2D kernel kz-major
   KernOct K;
   float* m = nullptr;
   float* t0 = nullptr;

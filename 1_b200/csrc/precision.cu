@@ -280,7 +280,7 @@ struct YconvTc {
   int64_t ktcs;        // component stride of kt
   const uint16_t* wf;  // forward W: hi, mid, lo tiles
   const uint16_t* wi;  // inverse W: hi, mid, lo tiles
-  const float2* tw;    // exp(-2 pi i t / 1024)
+  const float2* tw;    // [32][32]: tw[32 a + b] = exp(-2 pi i a b / 1024)
   int* err;
 };
 
@@ -368,16 +368,38 @@ __global__ void __launch_bounds__(YT, 1) k_yconv2d_tc(YconvTc a) {
   if (threadIdx.x == 0) dtc::mbar_init(&bar, 1);
   // the CTA's input, y < 512 of its 4 kz columns and 3 components, staged
   // through the W / twiddle area as lines stg[(c * 4 + kzl) * YSP + y]: a
-  // warp's load covers 8 y rows x 4 adjacent kz (32 contiguous bytes each)
+  // warp's load covers 8 y rows x 4 adjacent kz (32 contiguous bytes each).
+  // All of the CTA's global reads (input, W tiles, twiddles) are issued
+  // before the first store, so their latencies overlap.
   const int kz0 = blockIdx.x * YKZ;
+  const int skz = threadIdx.x & 3, sy = threadIdx.x >> 2;  // staging: kz, y offset (0 .. 63)
+  constexpr int NS = 3 * YN * YKZ / YT;                   // staged values per thread
+  constexpr int NW = 3 * YWB / 16 / YT;                   // 16-byte words of each W per thread
+  constexpr int NTW = YL / YT;                            // twiddles per thread
+  static_assert(NS * YT == 3 * YN * YKZ && NW * YT * 16 == 3 * YWB && NTW * YT == YL && YT / 4 * 8 == YN,
+                "load partition");
+  uint4 wreg[2 * NW];
+  float2 treg[NTW];
   {
-    float2* stg = reinterpret_cast<float2*>(wf);
-    for (int e = threadIdx.x; e < 3 * YN * YKZ; e += YT) {
-      const int kzl = e & 3, cy = e >> 2;
-      const int c = cy / YN, y = cy - c * YN;
-      const bool in = kz0 + kzl < HZ;
-      stg[(c * YKZ + kzl) * YSP + y] = in ? a.S[c * a.CS + (int64_t)y * HZ + kz0 + kzl] : make_float2(0.f, 0.f);
+    float2 sreg[NS];
+    const bool in = kz0 + skz < HZ;
+#pragma unroll
+    for (int u = 0; u < NS; u++) {  // component u / 8, y = 64 (u % 8) + sy
+      const int c = u >> 3, y = (u & 7) * 64 + sy;
+      sreg[u] = in ? a.S[c * a.CS + (int64_t)y * HZ + kz0 + skz] : make_float2(0.f, 0.f);
     }
+    const uint4* s0 = reinterpret_cast<const uint4*>(a.wf);
+    const uint4* s1 = reinterpret_cast<const uint4*>(a.wi);
+#pragma unroll
+    for (int u = 0; u < NW; u++) {
+      wreg[u] = __ldg(&s0[threadIdx.x + u * YT]);
+      wreg[NW + u] = __ldg(&s1[threadIdx.x + u * YT]);
+    }
+#pragma unroll
+    for (int u = 0; u < NTW; u++) treg[u] = __ldg(&a.tw[threadIdx.x + u * YT]);
+    float2* stg = reinterpret_cast<float2*>(wf);
+#pragma unroll
+    for (int u = 0; u < NS; u++) stg[((u >> 3) * YKZ + skz) * YSP + (u & 7) * 64 + sy] = sreg[u];
   }
   __syncthreads();
   // F1 operand, row (kz, n2 = lane): K = 64 c + 2 n1 (+1), value y[32 n1 + n2]
@@ -402,15 +424,15 @@ __global__ void __launch_bounds__(YT, 1) k_yconv2d_tc(YconvTc a) {
   }
   __syncthreads();  // staging read before the W tiles overwrite it
   {
-    const uint4* s0 = reinterpret_cast<const uint4*>(a.wf);
-    const uint4* s1 = reinterpret_cast<const uint4*>(a.wi);
     uint4* d0 = reinterpret_cast<uint4*>(wf);
     uint4* d1 = reinterpret_cast<uint4*>(wi);
-    for (int i = threadIdx.x; i < 3 * YWB / 16; i += YT) {
-      d0[i] = __ldg(&s0[i]);
-      d1[i] = __ldg(&s1[i]);
+#pragma unroll
+    for (int u = 0; u < NW; u++) {
+      d0[threadIdx.x + u * YT] = wreg[u];
+      d1[threadIdx.x + u * YT] = wreg[NW + u];
     }
-    for (int i = threadIdx.x; i < YL; i += YT) tw[i] = __ldg(&a.tw[i]);
+#pragma unroll
+    for (int u = 0; u < NTW; u++) tw[threadIdx.x + u * YT] = treg[u];
   }
   dtc::fence_async_smem();
   dtc::fence_before_sync();
@@ -455,7 +477,7 @@ __global__ void __launch_bounds__(YT, 1) k_yconv2d_tc(YconvTc a) {
 #pragma unroll
       for (int j = 0; j < 16; j++) {
         const int k1 = 16 * half + j;
-        const float2 w = tw[(n2 * k1) & (YL - 1)];
+        const float2 w = tw[32 * k1 + n2];  // lanes: consecutive n2
         const float zr = v[2 * j], zi = v[2 * j + 1];
         const float2 t = make_float2(fmaf(zr, w.x, -zi * w.y), fmaf(zr, w.y, zi * w.x));
         put_pair(xs, row0 + k1, 64 * c + 2 * n2, t);
@@ -515,7 +537,7 @@ __global__ void __launch_bounds__(YT, 1) k_yconv2d_tc(YconvTc a) {
 #pragma unroll
       for (int j = 0; j < 16; j++) {
         const int n2 = 16 * half + j;
-        const float2 w = tw[(n2 * k1) & (YL - 1)];
+        const float2 w = tw[32 * n2 + k1];  // lanes: consecutive k1
         const float zr = v[2 * j], zi = v[2 * j + 1];
         const float2 t = make_float2(fmaf(zr, w.x, zi * w.y), fmaf(zi, w.x, -zr * w.y));  // z conj(w)
         put_pair(xs, row0 + n2, 64 * c + 2 * k1, t);
@@ -542,10 +564,12 @@ __global__ void __launch_bounds__(YT, 1) k_yconv2d_tc(YconvTc a) {
   __syncthreads();
   if (ok) {
     const float2* stg = reinterpret_cast<const float2*>(xs);
-    for (int e = threadIdx.x; e < 3 * YN * YKZ; e += YT) {
-      const int kzl = e & 3, cy = e >> 2;
-      const int c = cy / YN, y = cy - c * YN;
-      if (kz0 + kzl < HZ) a.S[c * a.CS + (int64_t)y * HZ + kz0 + kzl] = stg[(c * YKZ + kzl) * YSP + y];
+    if (kz0 + skz < HZ) {
+#pragma unroll 8
+      for (int u = 0; u < NS; u++) {
+        const int c = u >> 3, y = (u & 7) * 64 + sy;
+        a.S[c * a.CS + (int64_t)y * HZ + kz0 + skz] = stg[(c * YKZ + skz) * YSP + y];
+      }
     }
   }
   if (!ok && threadIdx.x == 0) atomicExch(a.err, 1);
@@ -571,9 +595,9 @@ static int yconv2d_tc_prepare(const uint16_t** wf, const uint16_t** wi, float2**
   {
     std::lock_guard<std::mutex> lock(g_tw_mu);
     if (!g_tw1024[dev]) {
-      std::vector<float2> t(YL);
+      std::vector<float2> t(YL);  // W1024^(a b) for a, b < 32, row-major
       for (int i = 0; i < YL; i++) {
-        double ang = -2.0 * M_PI * i / YL;
+        double ang = -2.0 * M_PI * (double)(((i >> 5) * (i & 31)) % YL) / YL;
         t[i] = make_float2((float)cos(ang), (float)sin(ang));
       }
       if (cudaMalloc(&g_tw1024[dev], sizeof(float2) * YL) != cudaSuccess) {

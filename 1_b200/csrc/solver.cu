@@ -708,10 +708,15 @@ __global__ void k_finalize_accept(float* __restrict__ m, const float* __restrict
   }
 }
 
-// <m>: per-component sums in float64 (block reduction + one atomic per
-// block), divided by the cell count (simoutput.go:236, simget.go:32).
-__global__ void k_sum3(const float* __restrict__ m, int64_t n, double* __restrict__ acc) {
+// <m> in one launch (simoutput.go:236, simget.go:32): per-component sums in
+// float64 (block reduction + one atomic per block); the last block to
+// finish (counted on 'done') divides by the cell count, writes the three
+// values to 'out' (device memory, or page-locked host memory the kernel can
+// reach) and clears acc and done for the next call.
+__global__ void k_avg_m(const float* __restrict__ m, int64_t n, double* __restrict__ acc, unsigned int* done,
+                        float* __restrict__ out) {
   __shared__ double sh[3][32];
+  __shared__ bool last;
   double v[3] = {0.0, 0.0, 0.0};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     v[0] += m[i];
@@ -720,21 +725,30 @@ __global__ void k_sum3(const float* __restrict__ m, int64_t n, double* __restric
   }
   for (int c = 0; c < 3; c++)
     for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(0xffffffffu, v[c], o);
-  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
   if (l == 0)
     for (int c = 0; c < 3; c++) sh[c][w] = v[c];
   __syncthreads();
   if (w == 0) {
-    int nw = blockDim.x >> 5;
+    const int nw = blockDim.x >> 5;
     for (int c = 0; c < 3; c++) {
       double t = l < nw ? sh[c][l] : 0.0;
       for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
       if (l == 0) atomicAdd(&acc[c], t);
     }
+    if (l == 0) {
+      __threadfence();
+      last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
   }
-}
-__global__ void k_avg_finish(const double* __restrict__ acc, double n, float* __restrict__ out) {
-  if (threadIdx.x < 3) out[threadIdx.x] = (float)(acc[threadIdx.x] / n);
+  __syncthreads();
+  if (last && threadIdx.x < 3) {
+    __threadfence();
+    const double total = atomicAdd(&acc[threadIdx.x], 0.0);
+    out[threadIdx.x] = (float)(total / (double)n);
+    acc[threadIdx.x] = 0.0;
+    if (threadIdx.x == 0) *done = 0u;
+  }
 }
 
 int solver_grid_1d(int64_t n) {
@@ -1430,14 +1444,27 @@ extern "C" int mmx_solver_step(mmx_solver* s, int nsteps, cudaStream_t st) {
 
 extern "C" int mmx_solver_avg_m(mmx_solver* s, float* out3, int on_host, cudaStream_t st) {
   if (!s || !out3) { mmx_set_error("null argument"); return MMX_ERR_ARG; }
+  // scratch: float 4..6 the staging of a host result, 8..13 the float64
+  // sums, 14 the block counter (all zero between calls)
   double* acc = reinterpret_cast<double*>(s->scratch + 8);
-  float* res = s->scratch + 4;
-  MMX_TRY(cudaMemsetAsync(acc, 0, 3 * sizeof(double), st));
-  k_sum3<<<solver_grid_1d(s->n), 256, 0, st>>>(s->m, s->n, acc);
+  unsigned int* done = reinterpret_cast<unsigned int*>(s->scratch + 14);
+  float* dst = out3;
+  bool copy = false;
+  if (on_host) {
+    // page-locked host memory is written by the kernel itself; other host
+    // memory through the staging floats and a copy
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, out3) == cudaSuccess && pa.type == cudaMemoryTypeHost && pa.devicePointer) {
+      dst = static_cast<float*>(pa.devicePointer);
+    } else {
+      cudaGetLastError();  // an unregistered pointer is not an error here
+      dst = s->scratch + 4;
+      copy = true;
+    }
+  }
+  k_avg_m<<<solver_grid_1d(s->n), 256, 0, st>>>(s->m, s->n, acc, done, dst);
   MMX_TRY(cudaGetLastError());
-  k_avg_finish<<<1, 32, 0, st>>>(acc, (double)s->n, on_host ? res : out3);
-  MMX_TRY(cudaGetLastError());
-  if (on_host) MMX_TRY(cudaMemcpyAsync(out3, res, 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
+  if (copy) MMX_TRY(cudaMemcpyAsync(out3, dst, 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
   return MMX_OK;
 }
 

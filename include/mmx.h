@@ -103,9 +103,10 @@ int mmx_solver_field(mmx_solver* s, const float* m, float* h, cudaStream_t strea
 
 /* <m>: the average magnetisation per internal component (the table output
  * of src/go/sim/simoutput.go:236), summed in float64 on the device.  With
- * on_host != 0, out3 is a host pointer filled by an asynchronous copy on
- * 'stream' (pinned memory makes it truly asynchronous); else a device
- * pointer. */
+ * on_host != 0, out3 is a host pointer: page-locked memory is written by
+ * the reducing kernel itself (one launch, no copy), other host memory by a
+ * copy on 'stream'; else a device pointer.  Asynchronous: the values are
+ * there once 'stream' has reached this call. */
 int mmx_solver_avg_m(mmx_solver* s, float* out3, int on_host, cudaStream_t stream);
 
 /* Total energy of the resident m in internal units (multiply by the

@@ -238,3 +238,34 @@ def test_fused_heun_spectrum_reuse(eng, cuda):
     assert np.abs(b.get_m() - o.m()).max() < 1e-5
     a.close()
     b.close()
+
+
+def test_avg_m_host_pinned_device_vs_oracle(eng, cuda):
+    """<m> (mmx_solver_avg_m) into pageable host memory, page-locked host
+    memory (written by the reducing kernel itself) and device memory, called
+    several times in a row (the accumulators clear themselves), against the
+    FP64 oracle's <m> after the same Heun steps."""
+    torch = cuda
+    c = anis_cube_like((64, 32, 4))
+    kw = dict(solver="heun", dt=1e-14)
+    m = O.seeded_m(c["grid"], 8, "random")
+    o = O.OracleSim(O.make_cfg(**c, **kw), m, bits=64)
+    s = eng.Solver(eng.mmx_params(**c, **kw))
+    s.set_m(m)
+    s.normalize()
+    s.step(5)
+    o.steps(5)
+    ref = o.m().reshape(3, -1).mean(axis=1)
+    pinned = torch.zeros((4, 3), dtype=torch.float32).pin_memory()
+    dev = torch.zeros((4, 3), dtype=torch.float32, device="cuda")
+    got = []
+    for k in range(4):
+        got.append(s.avg_m())  # pageable: staged copy
+        s.avg_m(P(pinned[k]), True)
+        s.avg_m(P(dev[k]), False)
+    torch.cuda.synchronize()
+    got = np.array(got)
+    assert np.array_equal(got, pinned.numpy()) and np.array_equal(got, dev.cpu().numpy())
+    assert (got == got[0]).all()
+    assert np.abs(got[0] - ref).max() < 1e-6, (got[0], ref)
+    s.close()

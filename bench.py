@@ -313,6 +313,13 @@ def run_serve(args, name):
                                                                                if q["index"] == r["index"])),
                             "steps": r["steps"], "latency_ms": 1e3 * r["latency"], "converged": r["converged"]}
                            for r in srv["res"]]
+    by_kind = {}
+    for r in srv["res"]:
+        by_kind.setdefault(r["kind"], []).append(r)
+    line["served"]["by_kind"] = {k: {"requests": len(v), "converged": sum(1 for r in v if r["converged"]),
+                                     "p50_ms": 1e3 * pct([r["latency"] for r in v], 50),
+                                     "p99_ms": 1e3 * pct([r["latency"] for r in v], 99),
+                                     "steps": sum(r["steps"] for r in v)} for k, v in sorted(by_kind.items())}
     if world > 1:
         import torch.distributed as dist
         lines = [None] * world

@@ -175,7 +175,7 @@ static cudaError_t run_conv(const Launch& l, cudaStream_t st) {
   constexpr int TKP = conv_tkp(L);
   constexpr int NBF = TKP * (L / fwd_radix(L, n_stages(L) - 1));
   constexpr int T = NBF < 64 ? 64 : (NBF > 512 ? 512 : ((NBF + 31) / 32) * 32);
-  size_t smem = sizeof(float2) * (size_t)odd_pitch(3 * TKP) * L;
+  size_t smem = conv_smem(L);
   // variant 1: every instance of the launch has its data in the lower half
 #define KB_CONV_(D2, HALF)                                                                              \
   set_smem(kb_conv<L, TKP, T, D2, HALF>, smem);                                                         \

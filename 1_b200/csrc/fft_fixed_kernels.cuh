@@ -642,12 +642,24 @@ __host__ __device__ constexpr int fx_col_tk(int L) {
 __host__ __device__ constexpr int conv_tk_raw(int L) {
   return L >= 2048 ? 1 : (1365 / L > 32 ? 32 : (1365 / L < 1 ? 1 : 1365 / L));
 }
+// butterflies per column in the last forward stage (one thread each)
+__host__ __device__ constexpr int conv_bf(int L) { return L / fwd_radix(L, n_stages(L) - 1); }
+// Lines whose last stage has fewer than 8 butterflies per column (L = 2, 4,
+// 8, 16 in one stage; 6, 12 in two) take 128 / conv_bf columns, so that a
+// block still has 128 busy threads: a 16-column tile of L = 8 left 48 of
+// its 64 threads idle.
 __host__ __device__ constexpr int conv_tkp(int L) {
-  return conv_tk_raw(L) >= 16 ? 16
+  return conv_bf(L) < 8                   ? 128 / conv_bf(L)
+         : conv_tk_raw(L) >= 16 ? 16
          : conv_tk_raw(L) >= 8            ? 8
          : conv_tk_raw(L) >= 4            ? 4
          : conv_tk_raw(L) >= 2            ? 2
                                           : 1;
+}
+// shared-memory tile of a convolution block (none for one-stage lines,
+// whose butterflies stay in registers from load to store)
+__host__ __device__ constexpr size_t conv_smem(int L) {
+  return n_stages(L) == 1 ? 0 : sizeof(float2) * (size_t)odd_pitch(3 * conv_tkp(L)) * L;
 }
 __host__ __device__ constexpr int fx_threads(int elems) {
   return elems / 16 < 64 ? 64 : (elems / 16 > 512 ? 512 : ((elems / 16 + 31) / 32) * 32);
@@ -676,7 +688,7 @@ cudaError_t fx_launch_conv(const ConvArgs& a, cudaStream_t st) {
   // one thread per (column, radix-8 butterfly): it owns the three components
   constexpr int NBF = TKP * (L / fwd_radix(L, n_stages(L) - 1));
   constexpr int T = NBF < 64 ? 64 : (NBF > 512 ? 512 : ((NBF + 31) / 32) * 32);
-  size_t smem = sizeof(float2) * (size_t)odd_pitch(3 * TKP) * L;
+  size_t smem = conv_smem(L);
   if (2 * a.n_data == L) {
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(k_conv_fx<L, TKP, T, D2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

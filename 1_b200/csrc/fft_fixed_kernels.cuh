@@ -355,7 +355,12 @@ __device__ __forceinline__ void zr2c_body(const float* __restrict__ src, float2*
       if (l < nl) {
         const int64_t roff = roff_s[l];
         const int i0 = 2 * n;
-        if (COMB) {
+        if (COMB && vec2 && i0 + 1 < nreal) {
+          const float2 p = zcomb_value2(cb, dt, roff + i0);
+          *reinterpret_cast<float2*>(cb.out + roff + i0) = p;
+          a = p.x;
+          b = p.y;
+        } else if (COMB) {
           if (i0 < nreal) { a = zcomb_value(cb, dt, roff + i0); cb.out[roff + i0] = a; }
           if (i0 + 1 < nreal) { b = zcomb_value(cb, dt, roff + i0 + 1); cb.out[roff + i0 + 1] = b; }
         } else if (vec2 && i0 + 1 < nreal) {

@@ -74,6 +74,22 @@ __device__ __forceinline__ float zcomb_value(const ZComb& cb, float dt, int64_t 
   return q;
 }
 
+// The same for the two adjacent elements gi, gi + 1 (gi even, 8-byte
+// aligned rows): 8-byte loads, each component rounded as above.
+__device__ __forceinline__ float2 zcomb_value2(const ZComb& cb, float dt, int64_t gi) {
+  float2 q = __ldg(reinterpret_cast<const float2*>(cb.m0 + gi));
+#pragma unroll
+  for (int j = 0; j < ZCOMB_MAXK; j++) {
+    if (j >= cb.nk) break;
+    if (cb.a[j] == 0.f) continue;
+    const float f = __fmul_rn(dt, cb.a[j]);
+    const float2 kk = __ldg(reinterpret_cast<const float2*>(cb.k[j] + gi));
+    q.x = __fadd_rn(q.x, __fmul_rn(f, kk.x));
+    q.y = __fadd_rn(q.y, __fmul_rn(f, kk.y));
+  }
+  return q;
+}
+
 // Forward R2C rows.  Tile: 'lines' rows of M complex values, line-major.
 template <int THREADS, int EPT, bool POW2, bool COMB>
 __global__ void FFT_BOUNDS(THREADS) k_z_r2c(const float* __restrict__ src, float2* __restrict__ dst, ZPass z,

@@ -28,6 +28,7 @@
 #include "fft_generic.cuh"
 #include <assert.h>
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "fft_passes.cuh"
@@ -141,6 +142,14 @@ cudaStream_t gpu_getstream(void) {
 // ---------------------------------------------------------------------
 static unsigned long long g_usedmem = 0;
 static int g_stride_cache = -1;
+
+bool gk_sync_each_call() {
+  static const bool on = [] {
+    const char* e = getenv("MMX_GPUKERN_SYNC");
+    return e && e[0] && e[0] != '0';
+  }();
+  return on;
+}
 
 __global__ void k_zero(float* a, int64_t n) {
   GRID_STRIDE(i, n) a[i] = 0.f;

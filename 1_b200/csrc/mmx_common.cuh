@@ -25,7 +25,18 @@
 
 // The ABI is synchronous: every entry point waits for its work
 // (gpu_safe.h:41 gpu_sync after each launch).
-#define GK_SYNC() GK_CHECK(cudaDeviceSynchronize())
+// The reference synchronises the device after every primitive (gpu_sync,
+// gpu_safe.h:40-44).  Here a drop-in primitive returns once its work is
+// queued on the legacy default stream, which orders it before every later
+// primitive and every cudaMemcpy of the caller; a failure surfaces, and
+// aborts, at the next synchronising call (a host copy, a reduction, a free).
+// MMX_GPUKERN_SYNC=1 in the environment restores a device synchronisation
+// after every primitive.
+bool gk_sync_each_call();
+#define GK_SYNC()                                                    \
+  do {                                                               \
+    if (gk_sync_each_call()) GK_CHECK(cudaDeviceSynchronize());      \
+  } while (0)
 #define GK_LAUNCHED() GK_CHECK(cudaGetLastError())
 
 // Status codes of the extended (mmx_*) ABI; it never aborts.

@@ -495,8 +495,10 @@ def kernel_host(eng, torch, params):
 
 def time_driver(eng, torch, w, m0, libpath, steps=20, warmup=2):
     """Whole-grid steps per second of a libgpukern implementation driven by
-    the Go-driver restatement (libmmxdriver.so): every primitive call is
-    synchronous, as in the reference, so the wall clock around the steps is
+    the Go-driver restatement (libmmxdriver.so).  The reference's library
+    synchronises the device after every primitive; this library's
+    primitives return once queued on the default stream.  The wall clock
+    runs from a device synchronisation to one after the last step, so it is
     the device time plus the launch gaps the call sequence imposes."""
     kw = sim_kwargs(w)
     k6 = kernel_host(eng, torch, eng.mmx_params(**kw))
@@ -511,7 +513,8 @@ def time_driver(eng, torch, w, m0, libpath, steps=20, warmup=2):
     n = int(np.prod(w["grid"]))
     return {"value": n * steps / el, "unit": "cell-steps/s", "ms_per_step": 1e3 * el / steps, "steps": steps,
             "warmup": warmup, "library": os.path.relpath(libpath, ROOT),
-            "path": "Go-driver restatement (libmmxdriver.so) over the libgpukern C ABI, synchronous calls"}
+            "path": "Go-driver restatement (libmmxdriver.so) over the libgpukern C ABI, the call sequence of the "
+                    "unchanged Go front end"}
 
 
 def run_reference(args, w, name):

@@ -5,7 +5,10 @@
 #pragma once
 #include "llg_ops.cuh"
 
-enum { EPI_FIELD = 0, EPI_HEUN1 = 1, EPI_HEUN2 = 2, EPI_TORQUE = 3, EPI_RK = 4 };
+// EPI_RK64: EPI_RK with the adaptive solvers' embedded error vector formed
+// and normed in float64 (the precision form)
+enum { EPI_FIELD = 0, EPI_HEUN1 = 1, EPI_HEUN2 = 2, EPI_TORQUE = 3, EPI_RK = 4, EPI_RK64 = 5 };
+__host__ __device__ constexpr bool epi_rk(int mode) { return mode == EPI_RK || mode == EPI_RK64; }
 
 #define RK_MAXS 7
 struct RKCoef {
@@ -43,7 +46,7 @@ struct EpiArgs {
 template <int MODE>
 struct EpiIn {
   float m[3];
-  float a0[(MODE == EPI_HEUN2 || MODE == EPI_RK) ? 3 : 1];
+  float a0[(MODE == EPI_HEUN2 || epi_rk(MODE)) ? 3 : 1];
   float a1[MODE == EPI_HEUN2 ? 3 : 1];
 };
 
@@ -53,7 +56,7 @@ __device__ __forceinline__ void epi_load(const EpiArgs& ea, int64_t g, EpiIn<MOD
   in.m[0] = ea.m_in[g];
   in.m[1] = ea.m_in[n + g];
   in.m[2] = ea.m_in[2 * n + g];
-  if (MODE == EPI_HEUN2 || MODE == EPI_RK) {
+  if (MODE == EPI_HEUN2 || epi_rk(MODE)) {
     in.a0[0] = ea.aux0[g];
     in.a0[1] = ea.aux0[n + g];
     in.a0[2] = ea.aux0[2 * n + g];
@@ -88,7 +91,7 @@ __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float 
     const int64_t n = ea.n;
     float mx = in.m[0], my = in.m[1], mz = in.m[2];
     llg_local(ea.lf, mx, my, mz, hx, hy, hz);
-    if constexpr (MODE == EPI_RK || MODE == EPI_TORQUE) {
+    if constexpr (epi_rk(MODE) || MODE == EPI_TORQUE) {
       // energy density of the stage's m: -1/2 m.h_conv - m.Hext - 1/2 K (m.u)^2
       // = -1/2 m.(h + Hext) with h the full field (the anisotropy terms
       // cancel), summed in float64
@@ -146,7 +149,7 @@ __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float 
         float d2 = fabsf(FA(mz, FM(-1.f, nz)));
         lmax = fmaxf(lmax, fmaxf(d0, fmaxf(d1, d2)));
       }
-    } else if (MODE == EPI_RK) {
+    } else if (epi_rk(MODE)) {
       float kx = hx, ky = hy, kz = hz;
       float* kd = ea.out0;
       kd[g] = kx;
@@ -169,7 +172,24 @@ __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float 
         q[1] = FA(q[1], FM(c, k1));
         q[2] = FA(q[2], FM(c, k2));
       }
-      if (ea.rk.final_stage && ea.rk.adaptive) {
+      if (MODE == EPI_RK64 && ea.rk.final_stage && ea.rk.adaptive) {
+        // the embedded error vector sum_j (b_j - b*_j) dt k_j formed and
+        // normed in float64 from the float32 stage torques
+        double e0 = 0.0, e1 = 0.0, e2 = 0.0;
+#pragma unroll
+        for (int j = 0; j < RK_MAXS; j++) {
+          if (j >= ea.rk.nk) break;
+          const double w = ((double)ea.rk.a[j] - (double)ea.rk.b2[j]) * (double)dt;
+          if (w == 0.0) continue;
+          float k0, k1, k2;
+          if (j == ea.stage) { k0 = kx; k1 = ky; k2 = kz; }
+          else { k0 = ea.kbuf[j][g]; k1 = ea.kbuf[j][n + g]; k2 = ea.kbuf[j][2 * n + g]; }
+          e0 = fma(w, (double)k0, e0);
+          e1 = fma(w, (double)k1, e1);
+          e2 = fma(w, (double)k2, e2);
+        }
+        lmax = fmaxf(lmax, (float)fmax(fabs(e0), fmax(fabs(e1), fabs(e2))));
+      } else if (ea.rk.final_stage && ea.rk.adaptive) {
         float lo[3] = {in.a0[0], in.a0[1], in.a0[2]};
 #pragma unroll
         for (int j = 0; j < RK_MAXS; j++) {
@@ -200,11 +220,11 @@ __device__ __forceinline__ void epi_cell_in(const EpiArgs& ea, int64_t g, float 
 // for RK stages, the warp sums of the energy density into *ea.energy
 template <int MODE>
 __device__ __forceinline__ void epi_flush_max(const EpiArgs& ea, float lmax, double eacc = 0.0) {
-  if ((MODE == EPI_HEUN2 || MODE == EPI_RK || MODE == EPI_TORQUE) && ea.err) {
+  if ((MODE == EPI_HEUN2 || epi_rk(MODE) || MODE == EPI_TORQUE) && ea.err) {
     for (int o = 16; o > 0; o >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
     if ((threadIdx.x & 31) == 0) atomic_max_nonneg(ea.err, lmax);
   }
-  if constexpr (MODE == EPI_RK || MODE == EPI_TORQUE) {
+  if constexpr (epi_rk(MODE) || MODE == EPI_TORQUE) {
     if (ea.energy) {
       for (int o = 16; o > 0; o >>= 1) eacc += __shfl_xor_sync(0xffffffffu, eacc, o);
       if ((threadIdx.x & 31) == 0) atomicAdd(ea.energy, eacc);

@@ -683,6 +683,8 @@ static cudaError_t rk_stage(mmx_solver* s, int i, cudaStream_t st, float* dt_dev
     ea.rk.final_stage = 1;
     ea.rk.adaptive = s->adaptive;
     ea.err = s->adaptive ? s->scratch : nullptr;
+    // the precision form keeps float64 for the embedded error norm
+    if (s->p.precision && s->adaptive) return launch_zinv<EPI_RK64>(s, ea, st);
     return launch_zinv<EPI_RK>(s, ea, st);
   }
   ea.out0 = s->kb[i];

@@ -63,7 +63,8 @@ typedef struct mmx_params {
   int faithful;         /* 1: keep the reference's FSAL-after-reject reuse */
   int accuracy;         /* face-integral points per side (reference: 8) */
   int precision;        /* 0: FP32 transforms; 1: split-BF16 tensor-core DFT
-                           GEMMs for the Y convolution (2D films, Ny = 512) */
+                           GEMMs for the Y convolution (2D films, Ny = 512),
+                           and the adaptive solvers' error norm in float64 */
   float thermal_k;      /* thermal field (temperature.go:21-36): each RK step adds
                            sigma N(0,1) per cell and component to the field of
                            all its stages, sigma = sqrt(thermal_k / dt) with

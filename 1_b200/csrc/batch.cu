@@ -168,14 +168,14 @@ static cudaError_t run_col(const Launch& l, cudaStream_t st) {
 }
 template <int L>
 static int conv_tk() {
-  return conv_tkp(L);
+  return conv_tkp_narrow(L);
 }
 template <int L>
 static cudaError_t run_conv(const Launch& l, cudaStream_t st) {
-  constexpr int TKP = conv_tkp(L);
+  constexpr int TKP = conv_tkp_narrow(L);
   constexpr int NBF = TKP * (L / fwd_radix(L, n_stages(L) - 1));
   constexpr int T = NBF < 64 ? 64 : (NBF > 512 ? 512 : ((NBF + 31) / 32) * 32);
-  size_t smem = conv_smem(L);
+  size_t smem = conv_smem_tk(L, TKP);
   // variant 1: every instance of the launch has its data in the lower half
 #define KB_CONV_(D2, HALF)                                                                              \
   set_smem(kb_conv<L, TKP, T, D2, HALF>, smem);                                                         \

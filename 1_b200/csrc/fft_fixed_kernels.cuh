@@ -653,7 +653,7 @@ __host__ __device__ constexpr int conv_bf(int L) { return L / fwd_radix(L, n_sta
 // 8, 16 in one stage; 6, 12 in two) take 128 / conv_bf columns, so that a
 // block still has 128 busy threads: a 16-column tile of L = 8 left 48 of
 // its 64 threads idle.
-__host__ __device__ constexpr int conv_tkp(int L) {
+__host__ __device__ constexpr int conv_tkp_narrow(int L) {
   return conv_bf(L) < 8                   ? 128 / conv_bf(L)
          : conv_tk_raw(L) >= 16 ? 16
          : conv_tk_raw(L) >= 8            ? 8
@@ -661,11 +661,25 @@ __host__ __device__ constexpr int conv_tkp(int L) {
          : conv_tk_raw(L) >= 2            ? 2
                                           : 1;
 }
-// shared-memory tile of a convolution block (none for one-stage lines,
-// whose butterflies stay in registers from load to store)
-__host__ __device__ constexpr size_t conv_smem(int L) {
-  return n_stages(L) == 1 ? 0 : sizeof(float2) * (size_t)odd_pitch(3 * conv_tkp(L)) * L;
+// Single-grid passes: lines of 384 points and more also keep at least 4
+// adjacent columns (up to 512 threads), so that a warp's accesses cover 8
+// rows x 32 contiguous bytes of the spectrum and of the kernel; with one or
+// two columns every lane read its own row (the 512 x 512 film's FP32 Y
+// convolution: 45.8 -> 20.9 us).  The batch keeps the narrow tiles: its
+// instances hold few columns each, and more, smaller blocks measured faster
+// there.
+__host__ __device__ constexpr int conv_tkp(int L) {
+  return conv_tkp_narrow(L) >= 4 ? conv_tkp_narrow(L)
+         : 512 / conv_bf(L) >= 4 ? 4
+         : 512 / conv_bf(L) >= 2 ? 2
+                                 : 1;
 }
+// shared-memory tile of a convolution block of TK columns (none for
+// one-stage lines, whose butterflies stay in registers from load to store)
+__host__ __device__ constexpr size_t conv_smem_tk(int L, int TK) {
+  return n_stages(L) == 1 ? 0 : sizeof(float2) * (size_t)odd_pitch(3 * TK) * L;
+}
+__host__ __device__ constexpr size_t conv_smem(int L) { return conv_smem_tk(L, conv_tkp(L)); }
 __host__ __device__ constexpr int fx_threads(int elems) {
   return elems / 16 < 64 ? 64 : (elems / 16 > 512 ? 512 : ((elems / 16 + 31) / 32) * 32);
 }

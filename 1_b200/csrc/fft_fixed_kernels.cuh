@@ -145,8 +145,19 @@ using St3 = St<L, R, NS, TK, T, true>;  // (t, j) butterflies, components looped
 // HALF: the line holds data in its lower half only (n_data = L/2, the
 // open-boundary case): the first stage skips the zero half and the last
 // inverse stage computes only the stored half.
-template <int L, int TK, int T, bool D2, bool HALF>
+// STREAM: the spectrum is read and written with evict-first cache hints, so
+// that the kernel octant (read once for ky and once for P1 - ky, a pass
+// apart) stays in L2 for its second read.  Set for the single-grid 3D pass
+// only: there the X convolution gains more (75.3 -> 72.7 us on the 256 x 256
+// x 32 grid) than the inverse Y pass loses by reading its input from DRAM
+// (38.2 -> 39.2 us).
+template <int L, int TK, int T, bool D2, bool HALF, bool STREAM = false>
 __device__ __forceinline__ void conv_body(const ConvArgs& a, int bx) {
+  auto sload = [](const float2* p) -> float2 { return STREAM ? __ldcs(p) : *p; };
+  auto sstore = [](float2* p, float2 v) {
+    if (STREAM) __stcs(p, v);
+    else *p = v;
+  };
   __shared__ float2 tw[L];
   extern __shared__ float2 sm[];
   constexpr int NST = n_stages(L);
@@ -175,7 +186,7 @@ __device__ __forceinline__ void conv_body(const ConvArgs& a, int bx) {
 #pragma unroll
         for (int q = 0; q < R0; q++) {
           int idx = S0::in_idx(j, q);
-          v[i][c][q] = ((HALF ? q < R0 / 2 : idx < nd) && t < nc) ? a.S[c * a.CS + idx * a.stride + col0 + t]
+          v[i][c][q] = ((HALF ? q < R0 / 2 : idx < nd) && t < nc) ? sload(&a.S[c * a.CS + idx * a.stride + col0 + t])
                                                                   : make_float2(0.f, 0.f);
         }
         if (HALF) dft_half<R0>(v[i][c], false);
@@ -194,7 +205,7 @@ __device__ __forceinline__ void conv_body(const ConvArgs& a, int bx) {
 #pragma unroll
         for (int q = 0; q < R0; q++) {
           int idx = S0::in_idx(j, q);
-          u[i][c][q] = ((HALF ? q < R0 / 2 : idx < nd) && t < nc) ? a.S[c * a.CS + idx * a.stride + col0 + t]
+          u[i][c][q] = ((HALF ? q < R0 / 2 : idx < nd) && t < nc) ? sload(&a.S[c * a.CS + idx * a.stride + col0 + t])
                                                                   : make_float2(0.f, 0.f);
         }
         if (HALF) dft_half<R0>(u[i][c], false);
@@ -256,7 +267,7 @@ __device__ __forceinline__ void conv_body(const ConvArgs& a, int bx) {
 #pragma unroll
         for (int q = 0; q < RL; q++) {
           int idx = SL::out_idx(j, q);
-          if ((HALF ? q < RL / 2 : idx < nd) && t < nc) a.S[c * a.CS + idx * a.stride + col0 + t] = v[i][c][q];
+          if ((HALF ? q < RL / 2 : idx < nd) && t < nc) sstore(&a.S[c * a.CS + idx * a.stride + col0 + t], v[i][c][q]);
         }
       }
     }
@@ -296,7 +307,7 @@ __device__ __forceinline__ void conv_body(const ConvArgs& a, int bx) {
 #pragma unroll
         for (int q = 0; q < RI; q++) {
           int idx = SI::out_idx(j, q);
-          if ((HALF ? q < RI / 2 : idx < nd) && t < nc) a.S[c * a.CS + idx * a.stride + col0 + t] = w[q];
+          if ((HALF ? q < RI / 2 : idx < nd) && t < nc) sstore(&a.S[c * a.CS + idx * a.stride + col0 + t], w[q]);
         }
       }
     }
@@ -308,7 +319,7 @@ template <int L, int TK, int T, bool D2, bool HALF>
 // measured faster than the unconstrained 96-register build (5 blocks) and
 // than 7 or 8 blocks (register spills)
 __global__ void __launch_bounds__(T, (768 / T) > 0 ? (768 / T) : 1) k_conv_fx(ConvArgs a) {
-  conv_body<L, TK, T, D2, HALF>(a, blockIdx.x);
+  conv_body<L, TK, T, D2, HALF, !D2>(a, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------

@@ -269,3 +269,44 @@ def test_avg_m_host_pinned_device_vs_oracle(eng, cuda):
     assert (got == got[0]).all()
     assert np.abs(got[0] - ref).max() < 1e-6, (got[0], ref)
     s.close()
+
+
+_SYNC_CHILD = r"""
+import os, sys, importlib
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import oracle as O
+sys.path.insert(0, os.path.join(sys.argv[1], "tests"))
+from test_gpu_solver import anis_cube_like
+eng = importlib.import_module("1_b200")
+c = anis_cube_like((16, 8, 4))
+kw = dict(solver="heun", dt=1e-14)
+o32 = O.OracleSim(O.make_cfg(**c, **kw), O.seeded_m(c["grid"], 4, "random"), bits=32)
+Pd = tuple(2 * n if n > 1 else n for n in o32.N)
+cs = o32.internal_params()["cellsize"]
+k6 = O.face_kernel6(Pd, cs)
+O.add_exch6_kernel(Pd, cs, k6)
+d = eng.DriverSim(eng.driver_config(**c, **kw), o32.m(), k6)
+d.steps(10)
+np.save(sys.argv[2], d.m())
+"""
+
+
+def test_drop_in_sync_env_gives_identical_results(tmp_path):
+    """The drop-in primitives return once queued on the default stream;
+    MMX_GPUKERN_SYNC=1 restores a device synchronisation after every
+    primitive (the reference's behaviour).  The Go-driver call sequence
+    gives the same m bit for bit either way (each run in its own process,
+    since the setting is read once)."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = {}
+    for flag in ("0", "1"):
+        env = dict(os.environ, MMX_GPUKERN_SYNC=flag)
+        f = str(tmp_path / ("m%s.npy" % flag))
+        r = subprocess.run([sys.executable, "-c", _SYNC_CHILD, root, f], env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[flag] = np.load(f)
+    assert np.array_equal(out["0"], out["1"])
